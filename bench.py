@@ -1,0 +1,284 @@
+#!/usr/bin/env python
+"""Benchmark: solves/s at FP64 backward error on one B200, the single large system.
+
+Workload: one float64 system, n = 8192, nrhs = 16, A = U diag(s) V^T with U, V the Q factors
+of seeded 8192 x 8192 N(0,1) matrices and s log-spaced from 1 to 1e-4 (kappa = 1e4), B with
+N(0,1) entries. A "step" is one complete solve of that system through the library's C ABI
+(LU, pivot check, triangular solves and, for the mixed method, FP64 refinement to the
+backward-error target n * 2^-53). Inputs are generated on the GPU with torch's seeded
+generator (an 8192^2 QR in NumPy would take minutes); A is 512 MiB, larger than L2, so no
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU oracle (a C restatement of rustymath's LU solve; the Rust
+reference cannot be built here) on the host cores, on the same system.
+One JSON line on stdout (rank 0)."""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s at FP64 backward error: TC+refinement vs plain FP64 LU on one B200"
+WORKLOAD = "single system n=8192 nrhs=16, A=U diag(logspace(0,-4)) V^T (kappa=1e4), B~N(0,1)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=8192)
+    p.add_argument("--nrhs", type=int, default=16)
+    p.add_argument("--method", default="auto", choices=["auto", "plain", "mixed"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_system(n, nrhs, seed, device):
+    """A = U diag(s) V^T (U, V: Q of QR of seeded N(0,1) matrices; U first), B ~ N(0,1)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    u = torch.linalg.qr(torch.randn(n, n, generator=g, device=device, dtype=torch.float64)).Q
+    v = torch.linalg.qr(torch.randn(n, n, generator=g, device=device, dtype=torch.float64)).Q
+    s = torch.logspace(0, -4, n, device=device, dtype=torch.float64)
+    a = (u * s) @ v.T
+    b = torch.randn(n, nrhs, generator=g, device=device, dtype=torch.float64)
+    del u, v
+    return a.contiguous(), b.contiguous()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(a_host, b_host, threads=None):
+    """The oracle's solve (rustymath's algorithm restated in C) on this host's cores."""
+    from oracle import oracle as O
+    cores = threads or os.cpu_count()
+    O.set_threads(cores)
+    n, k = b_host.shape
+    t0 = time.perf_counter()
+    x = O.solve(a_host, b_host)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"1 full solve n={n} nrhs={k} (oracle lu_factor+lu_solve, OpenMP)", "seconds": dt}, x
+
+
+def gemm_peak_f64(torch, dev):
+    """Measured FP64 GEMM rate of cuBLAS (torch.matmul float64, 8192^3, best of 5)."""
+    n = 8192
+    a = torch.randn(n, n, device=dev, dtype=torch.float64)
+    b = torch.randn(n, n, device=dev, dtype=torch.float64)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def time_dgemm_update(torch, lib, dev, n, k=128, reps=10):
+    """One representative launch of the dominant kernel: the rank-128 trailing update."""
+    m = n - k
+    a = torch.randn(m, k, device=dev, dtype=torch.float64)
+    b = torch.randn(k, m, device=dev, dtype=torch.float64)
+    c = torch.randn(m, m, device=dev, dtype=torch.float64)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(3):
+        lib.rm_dgemm(0, 0, m, m, k, -1.0, a.data_ptr(), k, b.data_ptr(), m, 1.0, c.data_ptr(), m, s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        lib.rm_dgemm(0, 0, m, m, k, -1.0, a.data_ptr(), k, b.data_ptr(), m, 1.0, c.data_ptr(), m, s)
+    e1.record()
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    return 2.0 * m * m * k / t / 1e12, t
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+    dev = "cuda:0" if torch.cuda.is_available() else "cpu"
+    a, b = make_system(args.n, args.nrhs, 0, dev)
+    a_h, b_h = a.cpu().numpy(), b.cpu().numpy()
+    del a, b
+    from oracle import oracle as O
+    cores = os.cpu_count()
+    O.set_threads(cores)
+    for _ in range(max(0, min(args.warmup, 1))):
+        O.solve(a_h, b_h)
+    times = []
+    x = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        x = O.solve(a_h, b_h)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = args.steps / total
+    berr = O.backward_error(a_h, x, b_h)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "method": "oracle restatement of rustymath lu_factor + lu_solve"},
+            "backward_error": berr,
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full solves n={args.n} nrhs={args.nrhs}"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import rustymath_b200 as rb
+    from rustymath_b200 import _lib
+    lib = _lib.load()
+
+    n, k = args.n, args.nrhs
+    a, b = make_system(n, k, rank, dev)
+    x = torch.empty_like(b)
+    method = args.method if args.method != "auto" else "plain"
+    opts = rb.linalg._options(method)
+    rep = _lib.SolveReport()
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        st = lib.rm_dsolve(n, a.data_ptr(), b.data_ptr(), k, x.data_ptr(), ctypes.byref(opts), ctypes.byref(rep), sp)
+        _lib.check(st, "rm_dsolve")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = lib.rm_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    launches = (lib.rm_launch_count() - launches0) // max(args.steps, 1)
+    elapsed = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = world * args.steps / elapsed
+    berr = rep.backward_error
+    method_used = "plain FP64 LU" if rep.method_used == _lib.RM_METHOD_PLAIN_F64 else "FP32 LU + FP64 refinement"
+
+    # ---- end to end through the host API, pinned host buffers, copies inside the timed region
+    a_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    b_h = torch.empty((n, k), dtype=torch.float64, pin_memory=True)
+    x_h = torch.empty((n, k), dtype=torch.float64, pin_memory=True)
+    a_h.copy_(a)
+    b_h.copy_(b)
+    an, bn, xn = a_h.numpy(), b_h.numpy(), x_h.numpy()
+    e2e_steps = max(1, min(args.steps, 3))
+    lib.rm_dsolve_host(n, an.ctypes.data, bn.ctypes.data, k, xn.ctypes.data, ctypes.byref(opts), ctypes.byref(rep))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        st = lib.rm_dsolve_host(n, an.ctypes.data, bn.ctypes.data, k, xn.ctypes.data, ctypes.byref(opts),
+                                ctypes.byref(rep))
+        _lib.check(st, "rm_dsolve_host")
+    e2e_t = (time.perf_counter() - t0) / e2e_steps
+    e2e = {"value": world / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": (n * n + n * k) * 8,
+           "d2h_bytes_per_step": n * k * 8, "api": "rm_dsolve_host (pinned host buffers)"}
+
+    if rank == 0:
+        # ---- roofline of the dominant kernel (the FP64 DMMA trailing update)
+        peak64 = gemm_peak_f64(torch, dev)
+        achieved, t_launch = time_dgemm_update(torch, lib, dev, n)
+        roofline = {"bound": "tensor", "kernel": "dgemm_kernel<128x128> rank-128 update m=n=8064 k=128",
+                    "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                    "peak_source": "measured cuBLAS FP64 GEMM 8192^3 in this run (no FP64 figure in MEASURED_PEAKS.json)",
+                    "traffic": None}
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu, x_cpu = cpu_baseline(a_h.numpy(), b_h.numpy())
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if method == "plain" else "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "method": method_used, "n": n, "nrhs": k,
+                           "l2": "inputs larger than L2 (A is 512 MiB)", "parallelism": f"replicas x{world}"},
+                "backward_error": berr, "backward_error_target": n * 2.0 ** -53,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks.summary(), "tflops_lu": (2.0 / 3.0) * n ** 3 / (elapsed / args.steps) / 1e12 * world}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,116 @@
+/* rm_cuda.h: the C ABI of rustymath-b200, a B200 (sm_100a) implementation of rustymath's
+ * dense float64 linear-algebra path: GEMM, LU with partial pivoting, the triangular solves
+ * and the reusable factorization.
+ *
+ * The entry points replace these reference interfaces (paths within rustymath 0.1.66):
+ *  - rm_dgemm          : Accelerated::xgemm, core/src/linalg/accelerate.rs:211, reached from
+ *                        Tiled::gemm (core/src/linalg.rs:772-774) and PlusTimes.inner
+ *                        (core/src/linalg.rs:1119-1132). CBLAS row-major shape.
+ *  - rm_dlu_factor     : Factor::matrix_lu_into, core/src/linalg/factor.rs:87 (lu_factor,
+ *                        factor.rs:617-630), plus the pivot test of LuWork::regular
+ *                        (factor.rs:221-226).
+ *  - rm_dlu_solve      : Factor::matrix_lu_solve, factor.rs:89 (lu_solve, factor.rs:633-641).
+ *  - rm_dsolve         : solve, factor.rs:279 (LuWork::solve, factor.rs:207-209).
+ *
+ * Conventions (the reference's):
+ *  - matrices are row-major float64 with a leading dimension in items;
+ *  - LU factors are column-major: item (i, j) at factors[j*n + i] ("row j holds column j"),
+ *    unit L strictly below the diagonal, U on and above it;
+ *  - perm[i] is the row of the factored matrix that row i of L*U comes from.
+ * Pointers named d_* are device pointers and the call is asynchronous on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) unless it says it synchronises.
+ * Pointers named h_* are host pointers and the call returns when its results are in
+ * host memory. Every entry point returns an rm status code. Calls on different streams,
+ * from different threads, are independent.
+ */
+#ifndef RM_CUDA_H
+#define RM_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define RM_OK 0
+#define RM_BAD_ARG 1          /* a size, pointer, stride or option out of range */
+#define RM_NOT_REGULAR 2      /* a pivot at most eps*n*max|a|: the reference takes lstsq here */
+#define RM_CUDA_ERROR 3       /* a CUDA call failed; rm_last_error() has the message */
+#define RM_TIMEOUT 4          /* a bounded device-side wait gave up */
+#define RM_NO_CONVERGENCE 5   /* refinement did not reach the tolerance and fallback was off */
+#define RM_NO_DEVICE 6        /* no CUDA device of compute capability 10.0 */
+#define RM_OUT_OF_MEMORY 7
+
+#define RM_NO_TRANS 0
+#define RM_TRANS 1
+
+/* Factorization methods for rm_dsolve. */
+#define RM_METHOD_PLAIN_F64 0    /* LU in float64: the drop-in for rustymath's solve */
+#define RM_METHOD_F32_IR 1       /* LU in float32 (tensor-core trailing updates) + float64 refinement */
+
+typedef struct rm_solve_options {
+  int32_t method;          /* RM_METHOD_* */
+  int32_t max_iterations;  /* refinement steps before the fallback decision (default 30) */
+  int32_t gmres_restart;   /* GMRES-refinement restart length (default 20, as rustymath's GMRES) */
+  int32_t fallback;        /* 1: fall back to RM_METHOD_PLAIN_F64 when refinement fails */
+  double tolerance;        /* normwise backward error to reach; 0 means n * 2^-53 */
+} rm_solve_options;
+
+typedef struct rm_solve_report {
+  double backward_error;   /* max over columns of ||b-Ax||inf / (||A||inf ||x||inf + ||b||inf) */
+  int32_t iterations;      /* refinement steps taken (0 for the plain method) */
+  int32_t method_used;     /* the method whose result was returned */
+  int32_t fell_back;       /* 1 when the mixed method fell back to the plain one */
+  int32_t regular;         /* LuWork::regular's verdict on the factored matrix */
+} rm_solve_report;
+
+/* Library version (major*10000 + minor*100 + patch) and the text of a status code. */
+int rm_version(void);
+const char *rm_status_string(int status);
+/* Copies the calling thread's last error message into buf (always NUL-terminated). */
+int rm_last_error(char *buf, size_t len);
+/* Kernels this process has launched through the library so far (a diagnostic counter). */
+int64_t rm_launch_count(void);
+/* Number of CUDA devices usable by this library (compute capability 10.x). */
+int rm_device_count(int *count);
+
+/* C = alpha*op(A)*op(B) + beta*C, row-major, op(X) = X or X^T (trans* = RM_TRANS).
+ * op(A) is m x k, op(B) is k x n, C is m x n. Mirrors Accelerated::xgemm
+ * (core/src/linalg/accelerate.rs:211) with order fixed to row-major. */
+int rm_dgemm(int transa, int transb, int64_t m, int64_t n, int64_t k, double alpha,
+             const double *d_a, int64_t lda, const double *d_b, int64_t ldb, double beta,
+             double *d_c, int64_t ldc, void *stream);
+int rm_dgemm_host(int transa, int transb, int64_t m, int64_t n, int64_t k, double alpha,
+                  const double *h_a, int64_t lda, const double *h_b, int64_t ldb, double beta,
+                  double *h_c, int64_t ldc);
+
+/* LU with partial pivoting of the n x n row-major d_a into column-major d_factors and
+ * d_perm (int64), as lu_factor (core/src/linalg/factor.rs:617-630) gives them. When
+ * h_regular is not NULL the call synchronises and writes LuWork::regular's verdict
+ * (factor.rs:221-226): 1 when every |u_ii| > eps*n*max|a|. */
+int rm_dlu_factor(int64_t n, const double *d_a, double *d_factors, int64_t *d_perm,
+                  int32_t *h_regular, void *stream);
+int rm_dlu_factor_host(int64_t n, const double *h_a, double *h_factors, int64_t *h_perm,
+                       int32_t *h_regular);
+
+/* x = A^-1 b (trans = RM_NO_TRANS) or A^-T b (RM_TRANS) for the matrix the factors and
+ * perm describe; b and x are n x k row-major (they may alias). Mirrors lu_solve
+ * (core/src/linalg/factor.rs:633-641); the transposed form serves the adjoint. */
+int rm_dlu_solve(int64_t n, const double *d_factors, const int64_t *d_perm, const double *d_b,
+                 int64_t k, double *d_x, int trans, void *stream);
+int rm_dlu_solve_host(int64_t n, const double *h_factors, const int64_t *h_perm,
+                      const double *h_b, int64_t k, double *h_x, int trans);
+
+/* x = A^-1 b for the n x n row-major A and n x k row-major b, by the method in opts (NULL:
+ * plain float64). Returns RM_NOT_REGULAR, writing nothing to x, where rustymath's solve
+ * would take its least-squares route (factor.rs:207-209). Synchronises on `stream`. */
+int rm_dsolve(int64_t n, const double *d_a, const double *d_b, int64_t k, double *d_x,
+              const rm_solve_options *opts, rm_solve_report *report, void *stream);
+int rm_dsolve_host(int64_t n, const double *h_a, const double *h_b, int64_t k, double *h_x,
+                   const rm_solve_options *opts, rm_solve_report *report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

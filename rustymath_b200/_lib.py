@@ -1,0 +1,97 @@
+"""ctypes binding of librm_cuda.so (include/rm_cuda.h).
+
+The library is required: importing the compute functions without it raises, so no call
+can silently run anywhere but the B200 kernels."""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librm_cuda.so")
+
+RM_OK, RM_BAD_ARG, RM_NOT_REGULAR, RM_CUDA_ERROR = 0, 1, 2, 3
+RM_TIMEOUT, RM_NO_CONVERGENCE, RM_NO_DEVICE, RM_OUT_OF_MEMORY = 4, 5, 6, 7
+RM_METHOD_PLAIN_F64, RM_METHOD_F32_IR = 0, 1
+
+_i32, _i64, _f64, _p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class SolveOptions(ctypes.Structure):
+    _fields_ = [("method", _i32), ("max_iterations", _i32), ("gmres_restart", _i32), ("fallback", _i32),
+                ("tolerance", _f64)]
+
+
+class SolveReport(ctypes.Structure):
+    _fields_ = [("backward_error", _f64), ("iterations", _i32), ("method_used", _i32), ("fell_back", _i32),
+                ("regular", _i32)]
+
+
+# name -> (restype, argtypes); the set of exported entry points the header declares.
+SIGNATURES = {
+    "rm_version": (ctypes.c_int, []),
+    "rm_launch_count": (_i64, []),
+    "rm_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "rm_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
+    "rm_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    "rm_dgemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _i64, _i64, _f64, _p, _i64, _p, _i64, _f64, _p,
+                                _i64, _p]),
+    "rm_dgemm_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _i64, _i64, _f64, _p, _i64, _p, _i64, _f64,
+                                     _p, _i64]),
+    "rm_dlu_factor": (ctypes.c_int, [_i64, _p, _p, _p, ctypes.POINTER(_i32), _p]),
+    "rm_dlu_factor_host": (ctypes.c_int, [_i64, _p, _p, _p, ctypes.POINTER(_i32)]),
+    "rm_dlu_solve": (ctypes.c_int, [_i64, _p, _p, _p, _i64, _p, ctypes.c_int, _p]),
+    "rm_dlu_solve_host": (ctypes.c_int, [_i64, _p, _p, _p, _i64, _p, ctypes.c_int]),
+    "rm_dsolve": (ctypes.c_int, [_i64, _p, _p, _i64, _p, ctypes.POINTER(SolveOptions), ctypes.POINTER(SolveReport),
+                                 _p]),
+    "rm_dsolve_host": (ctypes.c_int, [_i64, _p, _p, _i64, _p, ctypes.POINTER(SolveOptions),
+                                      ctypes.POINTER(SolveReport)]),
+}
+
+
+class RmError(RuntimeError):
+    """A failed call into librm_cuda.so, with its status code."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+class NotRegular(ValueError):
+    """A pivot is at most eps*n*max|a|: rustymath's solve would take its least-squares route,
+    which this library does not provide."""
+
+
+_lib = None
+
+
+def load():
+    """The loaded library (built in-tree by rustymath_b200.build); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m rustymath_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    _lib = lib
+    return lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(512)
+    load().rm_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status, what):
+    if status == RM_OK:
+        return
+    text = load().rm_status_string(status).decode()
+    detail = last_error()
+    msg = f"{what}: {text}" + (f" ({detail})" if detail else "")
+    if status == RM_BAD_ARG:
+        raise ValueError(msg)
+    if status == RM_NOT_REGULAR:
+        raise NotRegular(msg)
+    raise RmError(status, msg)

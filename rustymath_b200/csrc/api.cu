@@ -1,0 +1,588 @@
+// The C ABI (include/rm_cuda.h): argument checks, scratch, and the call sequences of the
+// plain float64 path. Every entry point returns an rm status code; nothing here falls back
+// to the CPU.
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rm_internal.h"
+
+namespace rm {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+void set_last_message(const char* msg) { g_last_error = msg ? msg : ""; }
+
+void set_last_error(cudaError_t e, const char* what, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+  g_last_error = buf;
+}
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ------------------------------------------------------------------ device facts
+int device_sm_count() {
+  static std::mutex mu;
+  static std::vector<int> counts;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)counts.size() <= dev) counts.resize(dev + 1, 0);
+  if (counts[dev] == 0) {
+    int c = 0;
+    if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0) c = 148;
+    counts[dev] = c;
+  }
+  return counts[dev];
+}
+
+__device__ unsigned g_device_status;
+
+unsigned* device_status() {
+  static std::mutex mu;
+  static std::vector<unsigned*> ptrs;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_device_status) != cudaSuccess) return nullptr;
+    ptrs[dev] = static_cast<unsigned*>(p);
+  }
+  return ptrs[dev];
+}
+
+int take_device_status(cudaStream_t stream) {
+  unsigned* st = device_status();
+  if (!st) return RM_CUDA_ERROR;
+  unsigned h = 0;
+  RM_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream));
+  RM_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (h) {
+    RM_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), stream));
+    if (h & RM_DEV_TIMEOUT) {
+      set_last_message("a bounded device-side wait gave up");
+      return RM_TIMEOUT;
+    }
+    if (h & RM_DEV_BAD_INDEX) {
+      set_last_message("a row position is outside 0..n-1");
+      return RM_BAD_ARG;
+    }
+  }
+  return RM_OK;
+}
+
+// ------------------------------------------------------------------ scratch
+int scratch_alloc(void** p, size_t bytes, cudaStream_t stream) {
+  *p = nullptr;
+  if (bytes == 0) return RM_OK;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    // Keep freed scratch in the pool between calls instead of returning it to the driver.
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t threshold = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+  });
+  cudaError_t e = cudaMallocAsync(p, bytes, stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    set_last_message("device memory exhausted");
+    return RM_OUT_OF_MEMORY;
+  }
+  RM_CUDA_TRY(e);
+  return RM_OK;
+}
+
+void scratch_free(void* p, cudaStream_t stream) {
+  if (p) cudaFreeAsync(p, stream);
+}
+
+// Carves aligned sub-buffers out of one stream-ordered allocation.
+struct Arena {
+  std::vector<size_t> offsets;
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    const size_t off = total;
+    total = (total + bytes + 255) / 256 * 256;
+    return off;
+  }
+};
+
+struct Scratch {
+  void* base = nullptr;
+  cudaStream_t stream = nullptr;
+  ~Scratch() { scratch_free(base, stream); }
+  template <typename T>
+  T* at(size_t off) const {
+    return reinterpret_cast<T*>(static_cast<char*>(base) + off);
+  }
+};
+
+// ------------------------------------------------------------------ TMA descriptors
+int make_tensor_map_2d(CUtensorMap* map, const void* base, int elem_bytes, uint64_t inner, uint64_t outer,
+                       uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer, bool swizzle128) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!encode) {
+    set_last_message("cuTensorMapEncodeTiled is unavailable");
+    return RM_CUDA_ERROR;
+  }
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_stride_bytes & 15)) {
+    set_last_message("a TMA operand needs a 16-byte aligned base and row stride");
+    return RM_BAD_ARG;
+  }
+  CUtensorMapDataType dt = elem_bytes == 8   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                           : elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                           : elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                             : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  cuuint64_t dims[2] = {inner, std::max<uint64_t>(outer, 1)};
+  cuuint64_t strides[1] = {std::max<uint64_t>(row_stride_bytes, 16)};
+  cuuint32_t box[2] = {box_inner, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    set_last_message(buf);
+    return RM_CUDA_ERROR;
+  }
+  return RM_OK;
+}
+
+// ------------------------------------------------------------------ transpose
+__global__ void transpose_kernel(const double* __restrict__ src, int64_t lds, int64_t m, int64_t n,
+                                 double* __restrict__ dst, int64_t ldd) {
+  __shared__ double tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t i = i0 + r, j = j0 + threadIdx.x;
+    if (i < m && j < n) tile[r][threadIdx.x] = src[i * lds + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t j = j0 + r, i = i0 + threadIdx.x;
+    if (i < m && j < n) dst[j * ldd + i] = tile[threadIdx.x][r];
+  }
+}
+
+int transpose_f64(const double* src, int64_t lds, int64_t m, int64_t n, double* dst, int64_t ldd, cudaStream_t stream) {
+  if (m == 0 || n == 0) return RM_OK;
+  dim3 grid((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));
+  transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(src, lds, m, n, dst, ldd);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+// ------------------------------------------------------------------ plain solve pieces
+
+// The working copy of an n x n system: W (row-major, ld a multiple of 32), pivots, perm.
+struct LuBuffers {
+  size_t w, ipiv, perm, amax, flag, dinv, getrf, rowabs, berr;
+  int64_t ldw;
+};
+
+static LuBuffers plan_lu(Arena& arena, int64_t n) {
+  LuBuffers b;
+  b.ldw = round_up(std::max<int64_t>(n, 1), 32);
+  b.w = arena.add((size_t)n * b.ldw * sizeof(double));
+  b.ipiv = arena.add((size_t)n * sizeof(int64_t));
+  b.perm = arena.add((size_t)n * sizeof(int64_t));
+  b.amax = arena.add(sizeof(double));
+  b.flag = arena.add(sizeof(int32_t));
+  b.dinv = arena.add(diag_blocks_f64_bytes(n));
+  b.getrf = arena.add(getrf_f64_scratch_bytes(n));
+  b.rowabs = arena.add((size_t)n * sizeof(double));
+  b.berr = arena.add(2 * sizeof(double));
+  return b;
+}
+
+static cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+static int check_device() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_message("no CUDA device");
+    return RM_NO_DEVICE;
+  }
+  int major = 0;
+  RM_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (major != 10) {
+    set_last_message("librm_cuda needs a compute capability 10.x device (B200, sm_100a)");
+    return RM_NO_DEVICE;
+  }
+  return RM_OK;
+}
+
+}  // namespace rm
+
+using namespace rm;
+
+// ================================================================== C ABI
+extern "C" {
+
+int rm_version(void) { return 100; }
+
+int64_t rm_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+const char* rm_status_string(int status) {
+  switch (status) {
+    case RM_OK: return "ok";
+    case RM_BAD_ARG: return "bad argument";
+    case RM_NOT_REGULAR: return "matrix not regular (a pivot at most eps*n*max|a|)";
+    case RM_CUDA_ERROR: return "CUDA error";
+    case RM_TIMEOUT: return "device-side wait timed out";
+    case RM_NO_CONVERGENCE: return "refinement did not converge";
+    case RM_NO_DEVICE: return "no compute capability 10.x device";
+    case RM_OUT_OF_MEMORY: return "out of device memory";
+    default: return "unknown status";
+  }
+}
+
+int rm_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return RM_BAD_ARG;
+  const std::string& s = g_last_error;
+  const size_t n = std::min(len - 1, s.size());
+  memcpy(buf, s.data(), n);
+  buf[n] = 0;
+  return RM_OK;
+}
+
+int rm_device_count(int* count) {
+  if (!count) return RM_BAD_ARG;
+  *count = 0;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return RM_OK;
+  }
+  for (int d = 0; d < n; ++d) {
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) == cudaSuccess && major == 10) ++*count;
+  }
+  return RM_OK;
+}
+
+int rm_dgemm(int transa, int transb, int64_t m, int64_t n, int64_t k, double alpha, const double* d_a, int64_t lda,
+             const double* d_b, int64_t ldb, double beta, double* d_c, int64_t ldc, void* stream) {
+  if (m < 0 || n < 0 || k < 0 || (transa != 0 && transa != 1) || (transb != 0 && transb != 1)) return RM_BAD_ARG;
+  if (m == 0 || n == 0) return RM_OK;
+  const int64_t acols = transa ? m : k, bcols = transb ? k : n;
+  if (ldc < n || (k > 0 && (lda < std::max<int64_t>(acols, 1) || ldb < std::max<int64_t>(bcols, 1)))) return RM_BAD_ARG;
+  if (!d_c || (k > 0 && alpha != 0.0 && (!d_a || !d_b))) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  if (k == 0 || alpha == 0.0) return scale_device(d_c, ldc, m, n, beta, s);
+  // TMA wants 16-byte aligned rows: copy misaligned operands into padded buffers.
+  const double* a = d_a;
+  const double* b = d_b;
+  int64_t la = lda, lb = ldb;
+  Scratch sc;
+  sc.stream = s;
+  const bool fix_a = (reinterpret_cast<uintptr_t>(d_a) & 15) || (lda & 1);
+  const bool fix_b = (reinterpret_cast<uintptr_t>(d_b) & 15) || (ldb & 1);
+  if (fix_a || fix_b) {
+    Arena ar;
+    const int64_t arows = transa ? k : m, brows = transb ? n : k;
+    const int64_t pa = round_up(acols, 2), pb = round_up(bcols, 2);
+    const size_t oa = fix_a ? ar.add((size_t)arows * pa * sizeof(double)) : 0;
+    const size_t ob = fix_b ? ar.add((size_t)brows * pb * sizeof(double)) : 0;
+    RM_TRY(scratch_alloc(&sc.base, ar.total, s));
+    if (fix_a) {
+      RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<double>(oa), pa * sizeof(double), d_a, lda * sizeof(double),
+                                    acols * sizeof(double), arows, cudaMemcpyDeviceToDevice, s));
+      a = sc.at<double>(oa);
+      la = pa;
+    }
+    if (fix_b) {
+      RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<double>(ob), pb * sizeof(double), d_b, ldb * sizeof(double),
+                                    bcols * sizeof(double), brows, cudaMemcpyDeviceToDevice, s));
+      b = sc.at<double>(ob);
+      lb = pb;
+    }
+  }
+  return dgemm_device(transa != 0, transb != 0, m, n, k, alpha, a, la, b, lb, beta, d_c, ldc, device_status(), s);
+}
+
+int rm_dgemm_host(int transa, int transb, int64_t m, int64_t n, int64_t k, double alpha, const double* h_a,
+                  int64_t lda, const double* h_b, int64_t ldb, double beta, double* h_c, int64_t ldc) {
+  if (m < 0 || n < 0 || k < 0 || (transa != 0 && transa != 1) || (transb != 0 && transb != 1)) return RM_BAD_ARG;
+  if (m == 0 || n == 0) return RM_OK;
+  const int64_t arows = transa ? k : m, acols = transa ? m : k;
+  const int64_t brows = transb ? n : k, bcols = transb ? k : n;
+  if (ldc < n || (k > 0 && (lda < std::max<int64_t>(acols, 1) || ldb < std::max<int64_t>(bcols, 1)))) return RM_BAD_ARG;
+  if (!h_c || (k > 0 && (!h_a || !h_b))) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s;
+  RM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st = RM_OK;
+  {
+    Arena ar;
+    const int64_t pa = round_up(std::max<int64_t>(acols, 1), 2), pb = round_up(std::max<int64_t>(bcols, 1), 2);
+    const size_t oa = ar.add((size_t)arows * pa * sizeof(double));
+    const size_t ob = ar.add((size_t)brows * pb * sizeof(double));
+    const size_t oc = ar.add((size_t)m * n * sizeof(double));
+    Scratch sc;
+    sc.stream = s;
+    st = scratch_alloc(&sc.base, ar.total, s);
+    if (st == RM_OK) {
+      cudaError_t e = cudaSuccess;
+      if (k > 0) {
+        e = cudaMemcpy2DAsync(sc.at<double>(oa), pa * 8, h_a, lda * 8, acols * 8, arows, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpy2DAsync(sc.at<double>(ob), pb * 8, h_b, ldb * 8, bcols * 8, brows, cudaMemcpyHostToDevice, s);
+      }
+      if (e == cudaSuccess && beta != 0.0)
+        e = cudaMemcpy2DAsync(sc.at<double>(oc), n * 8, h_c, ldc * 8, n * 8, m, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) {
+        set_last_error(e, "host to device copy", __FILE__, __LINE__);
+        st = RM_CUDA_ERROR;
+      }
+      if (st == RM_OK)
+        st = rm_dgemm(transa, transb, m, n, k, alpha, sc.at<double>(oa), pa, sc.at<double>(ob), pb, beta,
+                      sc.at<double>(oc), n, s);
+      if (st == RM_OK) {
+        e = cudaMemcpy2DAsync(h_c, ldc * 8, sc.at<double>(oc), n * 8, n * 8, m, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) {
+          set_last_error(e, "device to host copy", __FILE__, __LINE__);
+          st = RM_CUDA_ERROR;
+        }
+      }
+    }
+  }
+  if (st == RM_OK) st = take_device_status(s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (st == RM_OK && e != cudaSuccess) {
+    set_last_error(e, "stream synchronize", __FILE__, __LINE__);
+    st = RM_CUDA_ERROR;
+  }
+  cudaStreamDestroy(s);
+  return st;
+}
+
+int rm_dlu_factor(int64_t n, const double* d_a, double* d_factors, int64_t* d_perm, int32_t* h_regular, void* stream) {
+  if (n < 0 || (n > 0 && (!d_a || !d_factors || !d_perm))) return RM_BAD_ARG;
+  if (h_regular) *h_regular = 0;
+  if (n == 0) return RM_OK;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  Arena ar;
+  LuBuffers lb = plan_lu(ar, n);
+  Scratch sc;
+  sc.stream = s;
+  RM_TRY(scratch_alloc(&sc.base, ar.total, s));
+  double* w = sc.at<double>(lb.w);
+  RM_TRY(load_matrix_f64(d_a, n, w, lb.ldw, n, sc.at<double>(lb.amax), s));
+  RM_TRY(getrf_f64(w, lb.ldw, n, sc.at<int64_t>(lb.ipiv), d_perm, sc.at<void>(lb.getrf), device_status(), s));
+  RM_TRY(store_factors_f64(w, lb.ldw, n, d_factors, s));
+  if (h_regular) {
+    RM_TRY(regular_flag_f64(w, lb.ldw, n, sc.at<double>(lb.amax), sc.at<int32_t>(lb.flag), s));
+    RM_CUDA_TRY(cudaMemcpyAsync(h_regular, sc.at<int32_t>(lb.flag), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RM_TRY(take_device_status(s));
+  }
+  return RM_OK;
+}
+
+int rm_dlu_factor_host(int64_t n, const double* h_a, double* h_factors, int64_t* h_perm, int32_t* h_regular) {
+  if (n < 0 || (n > 0 && (!h_a || !h_factors || !h_perm))) return RM_BAD_ARG;
+  if (h_regular) *h_regular = 0;
+  if (n == 0) return RM_OK;
+  RM_TRY(check_device());
+  cudaStream_t s;
+  RM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st;
+  {
+    Arena ar;
+    const size_t oa = ar.add((size_t)n * n * 8), of = ar.add((size_t)n * n * 8), op = ar.add((size_t)n * 8);
+    Scratch sc;
+    sc.stream = s;
+    st = scratch_alloc(&sc.base, ar.total, s);
+    if (st == RM_OK) {
+      cudaError_t e = cudaMemcpyAsync(sc.at<double>(oa), h_a, (size_t)n * n * 8, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) { set_last_error(e, "copy", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+      if (st == RM_OK) st = rm_dlu_factor(n, sc.at<double>(oa), sc.at<double>(of), sc.at<int64_t>(op), h_regular, s);
+      if (st == RM_OK) {
+        e = cudaMemcpyAsync(h_factors, sc.at<double>(of), (size_t)n * n * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_perm, sc.at<int64_t>(op), (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) { set_last_error(e, "copy", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+      }
+    }
+  }
+  if (st == RM_OK) st = take_device_status(s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return st;
+}
+
+int rm_dlu_solve(int64_t n, const double* d_factors, const int64_t* d_perm, const double* d_b, int64_t k, double* d_x,
+                 int trans, void* stream) {
+  if (n < 0 || k < 0 || (trans != 0 && trans != 1)) return RM_BAD_ARG;
+  if (n == 0 || k == 0) return RM_OK;
+  if (!d_factors || !d_perm || !d_b || !d_x) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  Arena ar;
+  const int64_t ldw = round_up(n, 32);
+  const size_t ow = ar.add((size_t)n * ldw * 8), od = ar.add(diag_blocks_f64_bytes(n)),
+               os = ar.add(getrs_f64_scratch_bytes(n, k));
+  Scratch sc;
+  sc.stream = s;
+  RM_TRY(scratch_alloc(&sc.base, ar.total, s));
+  double* w = sc.at<double>(ow);
+  // The factors are column-major: read row by row they are the transpose of L\U.
+  if (trans) {
+    RM_CUDA_TRY(cudaMemcpy2DAsync(w, ldw * 8, d_factors, n * 8, n * 8, n, cudaMemcpyDeviceToDevice, s));
+  } else {
+    RM_TRY(transpose_f64(d_factors, n, n, n, w, ldw, s));
+  }
+  RM_TRY(invert_diag_blocks_f64(w, ldw, n, sc.at<double>(od), /*lower_unit=*/!trans, /*upper_unit=*/trans != 0, s));
+  return getrs_f64(w, ldw, n, d_perm, sc.at<double>(od), d_b, k, k, d_x, k, sc.at<void>(os), device_status(), s,
+                   trans != 0);
+}
+
+int rm_dlu_solve_host(int64_t n, const double* h_factors, const int64_t* h_perm, const double* h_b, int64_t k,
+                      double* h_x, int trans) {
+  if (n < 0 || k < 0) return RM_BAD_ARG;
+  if (n == 0 || k == 0) return RM_OK;
+  if (!h_factors || !h_perm || !h_b || !h_x) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s;
+  RM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st;
+  {
+    Arena ar;
+    const size_t of = ar.add((size_t)n * n * 8), op = ar.add((size_t)n * 8), ob = ar.add((size_t)n * k * 8);
+    Scratch sc;
+    sc.stream = s;
+    st = scratch_alloc(&sc.base, ar.total, s);
+    if (st == RM_OK) {
+      cudaError_t e = cudaMemcpyAsync(sc.at<double>(of), h_factors, (size_t)n * n * 8, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(sc.at<int64_t>(op), h_perm, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(sc.at<double>(ob), h_b, (size_t)n * k * 8, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) { set_last_error(e, "copy", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+      if (st == RM_OK)
+        st = rm_dlu_solve(n, sc.at<double>(of), sc.at<int64_t>(op), sc.at<double>(ob), k, sc.at<double>(ob), trans, s);
+      if (st == RM_OK) {
+        e = cudaMemcpyAsync(h_x, sc.at<double>(ob), (size_t)n * k * 8, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) { set_last_error(e, "copy", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+      }
+    }
+  }
+  if (st == RM_OK) st = take_device_status(s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return st;
+}
+
+// The plain float64 solve: LU, LuWork::regular's test, then the two triangular solves.
+static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t k, double* d_x,
+                        rm_solve_report* report, cudaStream_t s) {
+  Arena ar;
+  LuBuffers lb = plan_lu(ar, n);
+  const size_t os = ar.add(getrs_f64_scratch_bytes(n, k));
+  const size_t orr = ar.add((size_t)n * k * 8);
+  Scratch sc;
+  sc.stream = s;
+  RM_TRY(scratch_alloc(&sc.base, ar.total, s));
+  double* w = sc.at<double>(lb.w);
+  RM_TRY(load_matrix_f64(d_a, n, w, lb.ldw, n, sc.at<double>(lb.amax), s));
+  RM_TRY(getrf_f64(w, lb.ldw, n, sc.at<int64_t>(lb.ipiv), sc.at<int64_t>(lb.perm), sc.at<void>(lb.getrf),
+                   device_status(), s));
+  RM_TRY(regular_flag_f64(w, lb.ldw, n, sc.at<double>(lb.amax), sc.at<int32_t>(lb.flag), s));
+  int32_t regular = 0;
+  RM_CUDA_TRY(cudaMemcpyAsync(&regular, sc.at<int32_t>(lb.flag), sizeof regular, cudaMemcpyDeviceToHost, s));
+  RM_TRY(take_device_status(s));
+  if (report) report->regular = regular;
+  if (!regular) {
+    set_last_message("a pivot is at most eps*n*max|a|; rustymath's solve takes least squares here");
+    return RM_NOT_REGULAR;
+  }
+  RM_TRY(invert_diag_blocks_f64(w, lb.ldw, n, sc.at<double>(lb.dinv), true, false, s));
+  RM_TRY(getrs_f64(w, lb.ldw, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k, sc.at<void>(os),
+                   device_status(), s));
+  if (report) {
+    double berr[2] = {0, 0};
+    RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(lb.rowabs), s));
+    RM_TRY(backward_error_f64(sc.at<double>(lb.rowabs), n, sc.at<double>(orr), k, d_x, k, d_b, k, k,
+                              sc.at<double>(lb.berr), s));
+    RM_CUDA_TRY(cudaMemcpyAsync(berr, sc.at<double>(lb.berr), sizeof berr, cudaMemcpyDeviceToHost, s));
+    RM_TRY(take_device_status(s));
+    report->backward_error = berr[0];
+    report->iterations = 0;
+    report->method_used = RM_METHOD_PLAIN_F64;
+    report->fell_back = 0;
+  }
+  return take_device_status(s);
+}
+
+int rm_dsolve(int64_t n, const double* d_a, const double* d_b, int64_t k, double* d_x, const rm_solve_options* opts,
+              rm_solve_report* report, void* stream) {
+  if (n < 0 || k < 0) return RM_BAD_ARG;
+  if (report) memset(report, 0, sizeof *report);
+  if (n == 0) {
+    set_last_message("an empty matrix is not regular; rustymath's solve takes least squares here");
+    return RM_NOT_REGULAR;
+  }
+  if (!d_a || (k > 0 && (!d_b || !d_x))) return RM_BAD_ARG;
+  const int method = opts ? opts->method : RM_METHOD_PLAIN_F64;
+  if (method != RM_METHOD_PLAIN_F64 && method != RM_METHOD_F32_IR) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  return dsolve_plain(n, d_a, d_b, k, d_x, report, s);
+}
+
+int rm_dsolve_host(int64_t n, const double* h_a, const double* h_b, int64_t k, double* h_x,
+                   const rm_solve_options* opts, rm_solve_report* report) {
+  if (n < 0 || k < 0) return RM_BAD_ARG;
+  if (report) memset(report, 0, sizeof *report);
+  if (n == 0) return rm_dsolve(0, nullptr, nullptr, k, nullptr, opts, report, nullptr);
+  if (!h_a || (k > 0 && (!h_b || !h_x))) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s;
+  RM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st;
+  {
+    Arena ar;
+    const size_t oa = ar.add((size_t)n * n * 8), ob = ar.add((size_t)n * k * 8), ox = ar.add((size_t)n * k * 8);
+    Scratch sc;
+    sc.stream = s;
+    st = scratch_alloc(&sc.base, ar.total, s);
+    if (st == RM_OK) {
+      cudaError_t e = cudaMemcpyAsync(sc.at<double>(oa), h_a, (size_t)n * n * 8, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess && k > 0) e = cudaMemcpyAsync(sc.at<double>(ob), h_b, (size_t)n * k * 8, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) { set_last_error(e, "copy", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+      if (st == RM_OK) st = rm_dsolve(n, sc.at<double>(oa), sc.at<double>(ob), k, sc.at<double>(ox), opts, report, s);
+      if (st == RM_OK && k > 0) {
+        e = cudaMemcpyAsync(h_x, sc.at<double>(ox), (size_t)n * k * 8, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) { set_last_error(e, "copy", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+      }
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (st == RM_OK && e != cudaSuccess) { set_last_error(e, "sync", __FILE__, __LINE__); st = RM_CUDA_ERROR; }
+  cudaStreamDestroy(s);
+  return st;
+}
+
+}  // extern "C"

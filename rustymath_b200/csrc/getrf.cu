@@ -1,0 +1,618 @@
+// LU with partial pivoting on the B200: the plain float64 path.
+//
+// Replaces lu_factor / lu_panel (core/src/linalg/factor.rs:580-630). The reference halves
+// columns recursively down to 16-column leaves on a column-major copy. Here the working
+// copy stays row-major (row swaps are contiguous and coalesced) and the factorization is
+// right-looking in blocks of kOuter columns, so the trailing update is a rank-128 FP64
+// product (compute-bound on DMMA) instead of the rank-16..n/2 products of the recursion:
+//
+//   for each block of kOuter columns at J0:
+//     for each 32-column leaf at j0 inside it:
+//       panel_kernel     : pivot search, row swap, scale and rank-1 updates of the leaf,
+//                          rows spread over a cluster of up to 16 CTAs' shared memory
+//       swap_trsm_kernel : the leaf's swaps on the block's other columns, and
+//                          U = L^-1 A for the leaf's rows of the block's later columns
+//       dgemm            : the block's later columns below the leaf -= L21 U12
+//     swap_trsm_kernel   : the block's swaps on every column outside it, and perm
+//     invert_unit_lower  : L11^-1 of the block's diagonal
+//     dgemm              : U12 = L11^-1 A12 (in place), then A22 -= L21 U12
+//
+// The pivot rule is the reference's `largest` (factor.rs:476): the first row of greatest
+// magnitude, NaN never chosen, the diagonal itself when every candidate is NaN; a zero
+// pivot leaves its column unreduced (factor.rs:606); `divide` multiplies by the
+// reciprocal unless the pivot is subnormal (factor.rs:506-508).
+#include <climits>
+
+#include "rm_internal.h"
+
+namespace rm {
+
+constexpr int kLeaf = 32;         // columns of a panel leaf
+constexpr int kOuter = 128;       // columns of an outer block (the trailing update's rank)
+constexpr int kPanelThreads = 256;
+constexpr int kPanelWarps = kPanelThreads / 32;
+constexpr int kPanelStride = kLeaf + 1;  // shared row stride (odd: conflict-free column reads)
+constexpr int kMaxCluster = 16;
+constexpr int kPanelSmemBudget = 200 * 1024;
+
+// ------------------------------------------------------------------ cluster helpers
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_nctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t map_rank(const void* p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, int v) {
+  asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ double ld_cluster_f64(uint32_t a) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_cluster_f32(uint32_t a) {
+  float v;
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T ld_cluster(uint32_t a) {
+  if constexpr (sizeof(T) == 8) return ld_cluster_f64(a);
+  else return ld_cluster_f32(a);
+}
+
+template <typename T>
+__device__ __forceinline__ T min_normal() {
+  if constexpr (sizeof(T) == 8) return 2.2250738585072014e-308;
+  else return 1.17549435e-38f;
+}
+
+// Keeps the larger magnitude, and on equal magnitudes the lower row (the first index).
+template <typename T>
+__device__ __forceinline__ void argmax_merge(T& v, int& i, T ov, int oi) {
+  if (ov > v || (ov == v && oi < i)) {
+    v = ov;
+    i = oi;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void warp_argmax(T& v, int& i) {
+#pragma unroll
+  for (int off = 16; off; off >>= 1) {
+    const T ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    argmax_merge(v, i, ov, oi);
+  }
+}
+
+template <typename T>
+struct PanelShared {
+  T red_v[kPanelWarps];
+  int red_i[kPanelWarps];
+  T slot_v[2][kMaxCluster];
+  int slot_i[2][kMaxCluster];
+  T cand[2][kLeaf];
+  T diag[2][kLeaf];
+  T piv[kLeaf];
+  T old[kLeaf];
+  int p;
+};
+
+// One leaf of up to kLeaf columns: rows j0..n-1, columns j0..j0+jb-1 of W. CTA `rank` of
+// the cluster holds rows [rank*rpc, (rank+1)*rpc) of the leaf (in shared memory when
+// IN_SMEM, else read and written in place); thread t owns the rows t, t+256, ...
+template <typename T, bool IN_SMEM>
+__global__ void __launch_bounds__(kPanelThreads)
+    panel_kernel(T* __restrict__ w, int64_t ldw, int n, int j0, int jb, int rpc, int64_t* __restrict__ ipiv) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int P = (int)cluster_nctarank();
+  const int rank = (int)cluster_ctarank();
+  const int M = n - j0;
+  const int base = rank * rpc;
+  const int cnt = max(0, min(rpc, M - base));
+  T* S = reinterpret_cast<T*>(smem);
+  const size_t rows_bytes = IN_SMEM ? ((size_t)rpc * kPanelStride * sizeof(T) + 15) / 16 * 16 : 0;
+  PanelShared<T>* sh = reinterpret_cast<PanelShared<T>*>(smem + rows_bytes);
+  T* g0 = w + (int64_t)(j0 + base) * ldw + j0;  // this CTA's first row, first leaf column
+
+  auto at = [&](int lr, int cc) -> T& {
+    if constexpr (IN_SMEM) return S[lr * kPanelStride + cc];
+    else return g0[(int64_t)lr * ldw + cc];
+  };
+
+  if constexpr (IN_SMEM) {
+    for (int e = tid; e < cnt * jb; e += kPanelThreads) {
+      const int lr = e / jb, cc = e - lr * jb;
+      S[lr * kPanelStride + cc] = g0[(int64_t)lr * ldw + cc];
+    }
+  }
+  __syncthreads();
+  if (P > 1) cluster_sync_all();  // every CTA of the cluster runs before any DSMEM access
+
+  for (int c = 0; c < jb; ++c) {
+    const int par = c & 1;
+    const int d = j0 + c;  // the diagonal row
+    // ---- this thread's candidate: first greatest magnitude among its rows >= d
+    T bv = T(-1);
+    int bi = INT_MAX;
+    for (int lr = tid; lr < cnt; lr += kPanelThreads) {
+      const int gi = j0 + base + lr;
+      if (gi >= d) {
+        const T v = fabs(at(lr, c));
+        if (v > bv) {  // NaN never compares greater
+          bv = v;
+          bi = gi;
+        }
+      }
+    }
+    warp_argmax(bv, bi);
+    if (lane == 0) {
+      sh->red_v[warp] = bv;
+      sh->red_i[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      bv = lane < kPanelWarps ? sh->red_v[lane] : T(-1);
+      bi = lane < kPanelWarps ? sh->red_i[lane] : INT_MAX;
+      warp_argmax(bv, bi);
+      if (lane < jb) {
+        if (bi != INT_MAX) sh->cand[par][lane] = at(bi - j0 - base, lane);
+        const int dl = d - j0 - base;
+        if (dl >= 0 && dl < cnt) sh->diag[par][lane] = at(dl, lane);
+      }
+      if (P > 1) {
+        if (lane < P) {
+          st_cluster(map_rank(&sh->slot_v[par][rank], lane), bv);
+          st_cluster(map_rank(&sh->slot_i[par][rank], lane), bi);
+        }
+      } else if (lane == 0) {
+        sh->slot_v[par][0] = bv;
+        sh->slot_i[par][0] = bi;
+      }
+    }
+    if (P > 1) cluster_sync_all();
+    else __syncthreads();
+    if (warp == 0) {
+      T v = lane < P ? sh->slot_v[par][lane] : T(-1);
+      int i = lane < P ? sh->slot_i[par][lane] : INT_MAX;
+      warp_argmax(v, i);
+      const int p = i == INT_MAX ? d : i;
+      const int owner_p = (p - j0) / rpc, owner_d = (d - j0) / rpc;
+      if (lane < jb) {
+        T dv, pv;
+        if (P > 1) {
+          dv = ld_cluster<T>(map_rank(&sh->diag[par][lane], owner_d));
+          pv = p == d ? dv : ld_cluster<T>(map_rank(&sh->cand[par][lane], owner_p));
+        } else {
+          dv = sh->diag[par][lane];
+          pv = p == d ? dv : sh->cand[par][lane];
+        }
+        sh->piv[lane] = pv;
+        sh->old[lane] = dv;
+      }
+      if (lane == 0) sh->p = p;
+    }
+    __syncthreads();
+    const int p = sh->p;
+    const T pivot = sh->piv[c];
+    if (p != d) {
+      const int dl = d - j0 - base, pl = p - j0 - base;
+      if (dl >= 0 && dl < cnt && dl % kPanelThreads == tid)
+        for (int cc = 0; cc < jb; ++cc) at(dl, cc) = sh->piv[cc];
+      if (pl >= 0 && pl < cnt && pl % kPanelThreads == tid)
+        for (int cc = 0; cc < jb; ++cc) at(pl, cc) = sh->old[cc];
+    }
+    if (pivot != T(0)) {
+      const bool sub = fabs(pivot) < min_normal<T>();
+      const T r = sub ? T(0) : T(1) / pivot;
+      for (int lr = tid; lr < cnt; lr += kPanelThreads) {
+        if (j0 + base + lr > d) {
+          T l = at(lr, c);
+          l = sub ? l / pivot : l * r;
+          at(lr, c) = l;
+          for (int cc = c + 1; cc < jb; ++cc) at(lr, cc) = fma(l, -sh->piv[cc], at(lr, cc));
+        }
+      }
+    }
+    if (rank == 0 && tid == 0) ipiv[d] = p;
+  }
+
+  if constexpr (IN_SMEM) {
+    __syncthreads();
+    for (int e = tid; e < cnt * jb; e += kPanelThreads) {
+      const int lr = e / jb, cc = e - lr * jb;
+      g0[(int64_t)lr * ldw + cc] = S[lr * kPanelStride + cc];
+    }
+  }
+  if (P > 1) cluster_sync_all();  // no CTA leaves while a peer may still read its memory
+}
+
+// ------------------------------------------------------------------ swaps + unit-lower solve
+constexpr int kSwapCols = 16;      // columns per CTA
+constexpr int kSwapThreads = 256;
+constexpr int kMaxSwaps = kOuter;  // pivots applied by one launch
+
+// Applies the swaps ipiv[j0..j0+jb) in order to the columns [lo1,hi1) and [lo2,hi2) of W.
+// With trsm_lo < trsm_hi, rows j0..j0+jb-1 of the columns in that range are then replaced
+// by L^-1 times them, L the unit lower triangle of W[j0.., j0..] (jb <= kLeaf). Block 0
+// also applies the swaps to perm when perm is not NULL.
+template <typename T>
+__global__ void __launch_bounds__(kSwapThreads)
+    swap_trsm_kernel(T* __restrict__ w, int64_t ldw, int j0, int jb, const int64_t* __restrict__ ipiv, int lo1,
+                     int hi1, int lo2, int hi2, int trsm_lo, int trsm_hi, int64_t* __restrict__ perm) {
+  __shared__ int pos[2 * kMaxSwaps], src[2 * kMaxSwaps];
+  __shared__ int count;
+  __shared__ T buf[2 * kMaxSwaps][kSwapCols + 1];
+  __shared__ T lblk[kLeaf][kLeaf + 1];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // ---- the net effect of the swaps: row pos[e] receives the old row src[e]
+  if (warp == 0) {
+    for (int q = lane; q < jb; q += 32) pos[q] = src[q] = j0 + q;
+    int cntE = jb;
+    for (int i = 0; i < jb; ++i) {
+      const int d = j0 + i, p = (int)ipiv[d];
+      if (p == d) continue;
+      int e;
+      if (p < j0 + jb) {
+        e = p - j0;
+      } else {
+        e = -1;
+        for (int b = jb; b < cntE && e < 0; b += 32) {
+          const unsigned hit = __ballot_sync(0xffffffffu, b + lane < cntE && pos[b + lane] == p);
+          if (hit) e = b + __ffs(hit) - 1;
+        }
+        if (e < 0) {
+          e = cntE;
+          if (lane == 0) pos[e] = src[e] = p;
+          ++cntE;
+        }
+        __syncwarp();
+      }
+      if (lane == 0) {
+        const int t = src[i];
+        src[i] = src[e];
+        src[e] = t;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) count = cntE;
+  }
+  __syncthreads();
+  const int E = count;
+
+  // ---- the columns of this CTA
+  const int chunks1 = (hi1 - lo1 + kSwapCols - 1) / kSwapCols;
+  int c0, c1;
+  if ((int)blockIdx.x < chunks1) {
+    c0 = lo1 + blockIdx.x * kSwapCols;
+    c1 = min(c0 + kSwapCols, hi1);
+  } else {
+    c0 = lo2 + (blockIdx.x - chunks1) * kSwapCols;
+    c1 = min(c0 + kSwapCols, hi2);
+  }
+  const int width = c1 - c0;
+
+  if (width > 0) {
+    for (int e = tid; e < E * kSwapCols; e += kSwapThreads) {
+      const int r = e / kSwapCols, cc = e - r * kSwapCols;
+      if (cc < width) buf[r][cc] = w[(int64_t)src[r] * ldw + c0 + cc];
+    }
+  }
+  const bool solve = width > 0 && trsm_lo < trsm_hi && c0 >= trsm_lo && c1 <= trsm_hi;
+  if (solve)
+    for (int e = tid; e < jb * kLeaf; e += kSwapThreads) {
+      const int r = e / kLeaf, cc = e - r * kLeaf;
+      lblk[r][cc] = cc < jb ? w[(int64_t)(j0 + r) * ldw + j0 + cc] : T(0);
+    }
+  __syncthreads();
+  if (solve) {
+    // one warp per column: lane r holds row r; row i is final once rows < i are removed
+    for (int cc = warp; cc < width; cc += kSwapThreads / 32) {
+      T x = lane < jb ? buf[lane][cc] : T(0);
+      for (int i = 0; i < jb; ++i) {
+        const T xi = __shfl_sync(0xffffffffu, x, i);
+        if (lane > i && lane < jb) x = fma(-lblk[lane][i], xi, x);
+      }
+      if (lane < jb) buf[lane][cc] = x;
+    }
+    __syncthreads();
+  }
+  if (width > 0) {
+    for (int e = tid; e < E * kSwapCols; e += kSwapThreads) {
+      const int r = e / kSwapCols, cc = e - r * kSwapCols;
+      if (cc < width && (pos[r] != src[r] || (solve && r < jb))) w[(int64_t)pos[r] * ldw + c0 + cc] = buf[r][cc];
+    }
+  }
+  if (perm != nullptr && blockIdx.x == 0) {
+    int64_t v[(2 * kMaxSwaps + kSwapThreads - 1) / kSwapThreads];
+#pragma unroll
+    for (int s = 0; s < (int)(sizeof(v) / sizeof(v[0])); ++s) {
+      const int e = tid + s * kSwapThreads;
+      v[s] = e < E ? perm[src[e]] : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < (int)(sizeof(v) / sizeof(v[0])); ++s) {
+      const int e = tid + s * kSwapThreads;
+      if (e < E) perm[pos[e]] = v[s];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ L11^-1 of an outer block
+// out (ld kOuter) = inverse of the unit lower triangle of W[j0..j0+nb, j0..j0+nb), nb <= kOuter.
+// Diagonal 32x32 blocks invert by column substitution (a warp each, a lane per column);
+// block (b, a) below them is -D_b^-1 * sum_{c=a..b-1} L_bc X_ca, in order of b - a. L is
+// read from W (it stays in L1/L2); X is built in `out`.
+template <typename T>
+__global__ void __launch_bounds__(256) invert_unit_lower_kernel(const T* __restrict__ w, int64_t ldw, int j0, int nb,
+                                                                T* __restrict__ out) {
+  __shared__ T tmp[kLeaf][kLeaf + 1];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const T* l = w + (int64_t)j0 * ldw + j0;
+  auto L = [&](int r, int c) -> T { return (r < nb && c < nb && c < r) ? l[(int64_t)r * ldw + c] : T(0); };
+  for (int e = tid; e < kOuter * kOuter; e += 256) out[e] = T(0);
+  __syncthreads();
+  const int nblk = (nb + kLeaf - 1) / kLeaf;
+  if (warp < nblk) {
+    const int b0 = warp * kLeaf;
+    // column `lane` of D^-1: x_i = -sum_{k<i} D_ik x_k for i > lane, x_lane = 1
+    T x[kLeaf];
+#pragma unroll
+    for (int i = 0; i < kLeaf; ++i) {
+      T s = i == lane ? T(1) : T(0);
+#pragma unroll
+      for (int k = 0; k < i; ++k) s = fma(-L(b0 + i, b0 + k), x[k], s);
+      x[i] = i < lane ? T(0) : s;
+    }
+#pragma unroll
+    for (int i = 0; i < kLeaf; ++i)
+      if (b0 + i < nb && b0 + lane < nb) out[(b0 + i) * kOuter + b0 + lane] = x[i];
+  }
+  __syncthreads();
+  for (int gap = 1; gap < nblk; ++gap) {
+    for (int a = 0; a + gap < nblk; ++a) {
+      const int b = a + gap, rb = b * kLeaf, ca = a * kLeaf;
+      // tmp = sum_{c=a..b-1} L_bc X_ca  (32x32)
+      for (int e = tid; e < kLeaf * kLeaf; e += 256) {
+        const int i = e / kLeaf, j = e % kLeaf;
+        T s = T(0);
+        for (int k = ca; k < rb; ++k) s = fma(L(rb + i, k), out[k * kOuter + ca + j], s);
+        tmp[i][j] = s;
+      }
+      __syncthreads();
+      // X_ba = -D_b^-1 tmp, with D_b^-1 (unit lower) in out's diagonal block b
+      for (int e = tid; e < kLeaf * kLeaf; e += 256) {
+        const int i = e / kLeaf, j = e % kLeaf;
+        T s = T(0);
+        for (int k = 0; k <= i; ++k) s = fma(out[(rb + i) * kOuter + rb + k], tmp[k][j], s);
+        if (rb + i < nb && ca + j < nb) out[(rb + i) * kOuter + ca + j] = -s;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ------------------------------------------------------------------ driver
+
+// The largest cluster (<= kMaxCluster CTAs of kPanelSmemBudget bytes) this device can place.
+template <typename T>
+static int panel_cluster_limit() {
+  static int limit = 0;
+  if (limit) return limit;
+  auto k = panel_kernel<T, true>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemBudget + 4096) != cudaSuccess ||
+      cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      cudaFuncSetAttribute(panel_kernel<T, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return limit = 8;
+  }
+  for (int P = kMaxCluster; P >= 1; P /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = P;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(P);
+    cfg.blockDim = dim3(kPanelThreads);
+    cfg.dynamicSmemBytes = kPanelSmemBudget;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k, &cfg) == cudaSuccess && clusters > 0) return limit = P;
+    cudaGetLastError();
+  }
+  return limit = 1;
+}
+
+template <typename T>
+static int launch_panel(T* w, int64_t ldw, int n, int j0, int jb, int64_t* ipiv, cudaStream_t stream) {
+  const int M = n - j0;
+  const size_t sh = (sizeof(PanelShared<T>) + 15) / 16 * 16;
+  const int rows_cap = (int)((kPanelSmemBudget - sh) / (kPanelStride * sizeof(T)));
+  const int pmax = panel_cluster_limit<T>();
+  int P = 1;
+  while (P < pmax && (M + P - 1) / P > rows_cap) P *= 2;
+  // spread tall leaves over more CTAs: about 2 rows per thread
+  while (P < pmax && (M + P - 1) / P > 2 * kPanelThreads) P *= 2;
+  const int rpc = (M + P - 1) / P;
+  const bool in_smem = rpc <= rows_cap;
+  const size_t smem = (in_smem ? ((size_t)rpc * kPanelStride * sizeof(T) + 15) / 16 * 16 : 0) + sh;
+
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = P;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(P);
+  cfg.blockDim = dim3(kPanelThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (in_smem) {
+    RM_CUDA_TRY(cudaLaunchKernelEx(&cfg, panel_kernel<T, true>, w, ldw, n, j0, jb, rpc, ipiv));
+  } else {
+    RM_CUDA_TRY(cudaLaunchKernelEx(&cfg, panel_kernel<T, false>, w, ldw, n, j0, jb, rpc, ipiv));
+  }
+  note_launch();
+  return RM_OK;
+}
+
+template <typename T>
+static int launch_swap(T* w, int64_t ldw, int j0, int jb, const int64_t* ipiv, int lo1, int hi1, int lo2, int hi2,
+                       int trsm_lo, int trsm_hi, int64_t* perm, cudaStream_t stream) {
+  hi1 = max(hi1, lo1);
+  hi2 = max(hi2, lo2);
+  const int chunks = (hi1 - lo1 + kSwapCols - 1) / kSwapCols + (hi2 - lo2 + kSwapCols - 1) / kSwapCols;
+  const int grid = max(chunks, perm ? 1 : 0);
+  if (grid == 0) return RM_OK;
+  swap_trsm_kernel<T><<<grid, kSwapThreads, 0, stream>>>(w, ldw, j0, jb, ipiv, lo1, hi1, lo2, hi2, trsm_lo, trsm_hi,
+                                                           perm);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+__global__ void iota_kernel(int64_t* perm, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    perm[i] = i;
+}
+
+size_t getrf_f64_scratch_bytes(int64_t n) { return (size_t)kOuter * kOuter * sizeof(double) + 256; }
+
+int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm, void* scratch, unsigned* status,
+              cudaStream_t stream) {
+  if (n64 <= 0) return RM_OK;
+  if (n64 > INT32_MAX / 2) return RM_BAD_ARG;
+  const int n = (int)n64;
+  double* linv = reinterpret_cast<double*>(scratch);
+  iota_kernel<<<std::max(1, std::min(n / 256 + 1, 1024)), 256, 0, stream>>>(perm, n);
+  RM_LAUNCHED();
+  for (int J0 = 0; J0 < n; J0 += kOuter) {
+    const int nb = std::min(kOuter, n - J0);
+    const int J1 = J0 + nb;
+    for (int j0 = J0; j0 < J1; j0 += kLeaf) {
+      const int jb = std::min(kLeaf, J1 - j0);
+      RM_TRY(launch_panel<double>(w, ldw, n, j0, jb, ipiv, stream));
+      // the leaf's swaps on the block's other columns; solve for its rows of later columns
+      RM_TRY(launch_swap<double>(w, ldw, j0, jb, ipiv, J0, j0, j0 + jb, J1, j0 + jb, J1, nullptr, stream));
+      if (j0 + jb < J1 && j0 + jb < n) {
+        const int64_t rows = n - (j0 + jb), cols = J1 - (j0 + jb);
+        RM_TRY(dgemm_device(false, false, rows, cols, jb, -1.0, w + (int64_t)(j0 + jb) * ldw + j0, ldw,
+                            w + (int64_t)j0 * ldw + j0 + jb, ldw, 1.0, w + (int64_t)(j0 + jb) * ldw + j0 + jb, ldw,
+                            status, stream));
+      }
+    }
+    // the block's swaps on every other column, and the row permutation
+    RM_TRY(launch_swap<double>(w, ldw, J0, nb, ipiv, 0, J0, J1, n, 0, 0, perm, stream));
+    if (J1 < n) {
+      invert_unit_lower_kernel<double><<<1, 256, 0, stream>>>(w, ldw, J0, nb, linv);
+      RM_LAUNCHED();
+      double* a12 = w + (int64_t)J0 * ldw + J1;
+      RM_TRY(dgemm_device(false, false, nb, n - J1, nb, 1.0, linv, kOuter, a12, ldw, 0.0, a12, ldw, status, stream,
+                          /*force_wide_m=*/true));
+      RM_TRY(dgemm_device(false, false, n - J1, n - J1, nb, -1.0, w + (int64_t)J1 * ldw + J0, ldw, a12, ldw, 1.0,
+                          w + (int64_t)J1 * ldw + J1, ldw, status, stream));
+    }
+  }
+  return RM_OK;
+}
+
+// ------------------------------------------------------------------ load / store / regular
+
+__global__ void load_matrix_kernel(const double* __restrict__ a, int64_t lda, double* __restrict__ w, int64_t ldw,
+                                   int64_t n, double* amax) {
+  double top = 0.0;
+  const int64_t total = n * ldw;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e / ldw, j = e - i * ldw;
+    double v = 0.0;
+    if (j < n) {
+      v = a[i * lda + j];
+      const double m = fabs(v);
+      if (m > top) top = m;
+    }
+    w[e] = v;
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) top = fmax(top, __shfl_xor_sync(0xffffffffu, top, off));
+  if ((threadIdx.x & 31) == 0 && top > 0.0)  // non-negative doubles order like their bits
+    atomicMax(reinterpret_cast<unsigned long long*>(amax), (unsigned long long)__double_as_longlong(top));
+}
+
+int load_matrix_f64(const double* a, int64_t lda, double* w, int64_t ldw, int64_t n, double* amax,
+                    cudaStream_t stream) {
+  RM_CUDA_TRY(cudaMemsetAsync(amax, 0, sizeof(double), stream));
+  if (n == 0) return RM_OK;
+  const int64_t total = n * ldw;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 8 * device_sm_count());
+  load_matrix_kernel<<<blocks, 256, 0, stream>>>(a, lda, w, ldw, n, amax);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+// factors[j*n + i] = W[i][j]: a 32x32-tiled transpose through shared memory
+__global__ void store_factors_kernel(const double* __restrict__ w, int64_t ldw, int64_t n, double* __restrict__ f) {
+  __shared__ double tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t i = i0 + r, j = j0 + threadIdx.x;
+    if (i < n && j < n) tile[r][threadIdx.x] = w[i * ldw + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t j = j0 + r, i = i0 + threadIdx.x;
+    if (i < n && j < n) f[j * n + i] = tile[threadIdx.x][r];
+  }
+}
+
+int store_factors_f64(const double* w, int64_t ldw, int64_t n, double* factors, cudaStream_t stream) {
+  if (n == 0) return RM_OK;
+  dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
+  store_factors_kernel<<<grid, dim3(32, 8), 0, stream>>>(w, ldw, n, factors);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+__global__ void regular_kernel(const double* __restrict__ w, int64_t ldw, int64_t n, const double* amax,
+                               int32_t* flag) {
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  const double negligible = 2.220446049250313e-16 * (double)n * *amax;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+    if (fabs(w[i * ldw + i]) <= negligible) bad = 1;  // NaN compares false: a NaN pivot is regular
+  __syncthreads();
+  if (threadIdx.x == 0) *flag = (n > 0 && !bad) ? 1 : 0;
+}
+
+int regular_flag_f64(const double* w, int64_t ldw, int64_t n, const double* amax, int32_t* flag,
+                     cudaStream_t stream) {
+  regular_kernel<<<1, 1024, 0, stream>>>(w, ldw, n, amax, flag);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+}  // namespace rm

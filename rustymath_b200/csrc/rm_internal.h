@@ -1,0 +1,74 @@
+// Internal interfaces between the CUDA translation units of librm_cuda.so.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+
+#include "rm_common.cuh"
+
+namespace rm {
+
+// ---------------------------------------------------------------- GEMM (dgemm.cu)
+// C = alpha*op(A)*op(B) + beta*C, row-major; a, b 16-byte aligned with even lda, ldb.
+// `force_wide_m` picks the 128-row tile whatever the size, which makes a product whose
+// m <= 128 read each column block of B in one CTA (so B may alias C).
+int dgemm_device(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* a, int64_t lda,
+                 const double* b, int64_t ldb, double beta, double* c, int64_t ldc, unsigned* status,
+                 cudaStream_t stream, bool force_wide_m = false);
+int scale_device(double* c, int64_t ldc, int64_t m, int64_t n, double beta, cudaStream_t stream);
+
+// ---------------------------------------------------------------- LU (getrf.cu)
+// Row-major working matrix W (n rows, ldw >= n, ldw % 32 == 0, 16-byte aligned). On return
+// W holds L\U of P*A row by row, ipiv[c] is the row swapped with row c (absolute) and
+// perm[i] the source row of row i. `scratch` holds getrf_f64_scratch_bytes(n) bytes.
+size_t getrf_f64_scratch_bytes(int64_t n);
+int getrf_f64(double* w, int64_t ldw, int64_t n, int64_t* ipiv, int64_t* perm, void* scratch, unsigned* status,
+              cudaStream_t stream);
+
+// Copies the row-major n x n `a` (lda) into W (ldw), zeroing W's padding columns, and
+// records max |a_ij| (NaN ignored) into *amax (device).
+int load_matrix_f64(const double* a, int64_t lda, double* w, int64_t ldw, int64_t n, double* amax,
+                    cudaStream_t stream);
+// Writes the column-major factors (item (i,j) at f[j*n+i]) from the row-major W.
+int store_factors_f64(const double* w, int64_t ldw, int64_t n, double* factors, cudaStream_t stream);
+// *flag = 1 when every |u_ii| > eps*n*amax (LuWork::regular), else 0.
+int regular_flag_f64(const double* w, int64_t ldw, int64_t n, const double* amax, int32_t* flag,
+                     cudaStream_t stream);
+
+// ---------------------------------------------------------------- solves (getrs.cu)
+size_t getrs_f64_scratch_bytes(int64_t n, int64_t k);
+// trans == false: x = (P^T L U)^-1 b, w the row-major L\U (W after getrf_f64).
+// trans == true : x = (P^T L U)^-T b, w the row-major transpose of L\U (the column-major
+//                 factors read row by row).
+// b, x row-major n x k (may alias). `dinv` holds the inverted diagonal blocks of w's two
+// triangles from invert_diag_blocks_f64(w, ..., lower_unit = !trans, upper_unit = trans).
+int getrs_f64(const double* w, int64_t ldw, int64_t n, const int64_t* perm, const double* dinv, const double* b,
+              int64_t ldb, int64_t k, double* x, int64_t ldx, void* scratch, unsigned* status, cudaStream_t stream,
+              bool trans = false);
+size_t diag_blocks_f64_bytes(int64_t n);
+int invert_diag_blocks_f64(const double* w, int64_t ldw, int64_t n, double* dinv, bool lower_unit, bool upper_unit,
+                           cudaStream_t stream);
+
+// ---------------------------------------------------------------- residual (residual.cu)
+// r = b - A x (FP64); rowabs[i] = sum_j |a_ij| when rowabs is not NULL.
+int residual_f64(const double* a, int64_t lda, int64_t n, const double* x, int64_t ldx, const double* b, int64_t ldb,
+                 int64_t k, double* r, int64_t ldr, double* rowabs, cudaStream_t stream);
+// out[0] = normwise backward error (max over columns), out[1] = ||A||_inf.
+int backward_error_f64(const double* rowabs, int64_t n, const double* r, int64_t ldr, const double* x, int64_t ldx,
+                       const double* b, int64_t ldb, int64_t k, double* out, cudaStream_t stream);
+
+// dst[j*ldd + i] = src[i*lds + j] for an m x n row-major src.
+int transpose_f64(const double* src, int64_t lds, int64_t m, int64_t n, double* dst, int64_t ldd, cudaStream_t stream);
+
+// The device-wide sticky status word (RM_DEV_* bits) of the current device.
+unsigned* device_status();
+// Reads and clears the current device's status word (synchronises `stream`); maps bits to
+// an rm status code.
+int take_device_status(cudaStream_t stream);
+
+// ---------------------------------------------------------------- helpers (api.cu)
+int64_t round_up(int64_t x, int64_t m);
+// Stream-ordered scratch allocation from the device's default pool.
+int scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
+void scratch_free(void* p, cudaStream_t stream);
+
+}  // namespace rm
