@@ -42,6 +42,8 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--method", default="auto", choices=["auto", "plain", "mixed"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--solve-only", action="store_true",
+                   help="only the timed solves (for profiling): no e2e, roofline or CPU legs")
     return p.parse_args()
 
 
@@ -235,6 +237,15 @@ def main():
     value = world * args.steps / elapsed
     berr = rep.backward_error
     method_used = "plain FP64 LU" if rep.method_used == _lib.RM_METHOD_PLAIN_F64 else "FP32 LU + FP64 refinement"
+
+    if args.solve_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "n": n, "nrhs": k,
+                              "ms_per_step": 1e3 * elapsed / args.steps, "backward_error": rep.backward_error,
+                              "method": method_used, "gpu_launches": int(launches)}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # ---- end to end through the host API, pinned host buffers, copies inside the timed region
     a_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)

@@ -226,9 +226,16 @@ class Lu(NamedTuple):
         return _stack(cells, _is_torch(f))
 
     def determinant(self):
-        "The determinant from these factors"
-        sign, log = self._signs()
-        return sign * _exp(log)
+        "The determinant from these factors: U's diagonal product, negated for an odd p (factor.rs:174-176)"
+        f, p = self.factors, self.p
+        if _is_torch(f):
+            return _torch().prod(_torch().diagonal(f, dim1=-2, dim2=-1), -1) * _parity(p)
+        d = np.diagonal(f, axis1=-2, axis2=-1)
+        prod = np.ones(d.shape[:-1])
+        for i in range(d.shape[-1]):  # in order, as the reference folds it
+            prod = prod * d[..., i]
+        out = prod * _parity(p)
+        return float(out) if np.ndim(out) == 0 else out
 
     def log_determinant(self):
         "The determinant's sign and the natural logarithm of its magnitude, from these factors"
@@ -251,10 +258,6 @@ class Lu(NamedTuple):
         if np.ndim(sign) == 0:
             return float(sign), float(log)
         return sign, log
-
-
-def _exp(x):
-    return _torch().exp(x) if _is_torch(x) else np.exp(x)
 
 
 def _parity(p):
