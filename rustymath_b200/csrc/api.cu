@@ -211,7 +211,7 @@ static LuBuffers plan_lu(Arena& arena, int64_t n) {
   b.flag = arena.add(sizeof(int32_t));
   b.dinv = arena.add(diag_blocks_f64_bytes(n));
   b.getrf = arena.add(getrf_f64_scratch_bytes(n));
-  b.rowabs = arena.add((size_t)n * sizeof(double));
+  b.rowabs = arena.add(sizeof(double));
   b.berr = arena.add(2 * sizeof(double));
   return b;
 }
@@ -443,22 +443,15 @@ int rm_dlu_solve(int64_t n, const double* d_factors, const int64_t* d_perm, cons
   RM_TRY(check_device());
   cudaStream_t s = as_stream(stream);
   Arena ar;
-  const int64_t ldw = round_up(n, 32);
-  const size_t ow = ar.add((size_t)n * ldw * 8), od = ar.add(diag_blocks_f64_bytes(n)),
-               os = ar.add(getrs_f64_scratch_bytes(n, k));
+  const size_t od = ar.add(diag_blocks_f64_bytes(n)), os = ar.add(getrs_f64_scratch_bytes(n, k));
   Scratch sc;
   sc.stream = s;
   RM_TRY(scratch_alloc(&sc.base, ar.total, s));
-  double* w = sc.at<double>(ow);
-  // The factors are column-major: read row by row they are the transpose of L\U.
-  if (trans) {
-    RM_CUDA_TRY(cudaMemcpy2DAsync(w, ldw * 8, d_factors, n * 8, n * 8, n, cudaMemcpyDeviceToDevice, s));
-  } else {
-    RM_TRY(transpose_f64(d_factors, n, n, n, w, ldw, s));
-  }
-  RM_TRY(invert_diag_blocks_f64(w, ldw, n, sc.at<double>(od), /*lower_unit=*/!trans, /*upper_unit=*/trans != 0, s));
-  return getrs_f64(w, ldw, n, d_perm, sc.at<double>(od), d_b, k, k, d_x, k, sc.at<void>(os), device_status(), s,
-                   trans != 0);
+  // The factors are column-major (rustymath's order); the kernels read them in place.
+  const DiagBlockArgs da = diag_block_args(trans != 0, true);
+  RM_TRY(invert_diag_blocks_f64(d_factors, n, da.colmajor, n, sc.at<double>(od), da.lower_unit, da.upper_unit, s));
+  return getrs_f64(d_factors, n, true, n, d_perm, sc.at<double>(od), d_b, k, k, d_x, k, sc.at<void>(os),
+                   device_status(), s, trans != 0);
 }
 
 int rm_dlu_solve_host(int64_t n, const double* h_factors, const int64_t* h_perm, const double* h_b, int64_t k,
@@ -502,6 +495,7 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   LuBuffers lb = plan_lu(ar, n);
   const size_t os = ar.add(getrs_f64_scratch_bytes(n, k));
   const size_t orr = ar.add((size_t)n * k * 8);
+  const size_t onorm = ar.add(residual_norms_bytes(k));
   Scratch sc;
   sc.stream = s;
   RM_TRY(scratch_alloc(&sc.base, ar.total, s));
@@ -518,14 +512,13 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
     set_last_message("a pivot is at most eps*n*max|a|; rustymath's solve takes least squares here");
     return RM_NOT_REGULAR;
   }
-  RM_TRY(invert_diag_blocks_f64(w, lb.ldw, n, sc.at<double>(lb.dinv), true, false, s));
-  RM_TRY(getrs_f64(w, lb.ldw, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k, sc.at<void>(os),
-                   device_status(), s));
+  RM_TRY(invert_diag_blocks_f64(w, lb.ldw, false, n, sc.at<double>(lb.dinv), true, false, s));
+  RM_TRY(getrs_f64(w, lb.ldw, false, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k,
+                   sc.at<void>(os), device_status(), s));
   if (report) {
     double berr[2] = {0, 0};
-    RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(lb.rowabs), s));
-    RM_TRY(backward_error_f64(sc.at<double>(lb.rowabs), n, sc.at<double>(orr), k, d_x, k, d_b, k, k,
-                              sc.at<double>(lb.berr), s));
+    RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
+    RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(lb.berr), s));
     RM_CUDA_TRY(cudaMemcpyAsync(berr, sc.at<double>(lb.berr), sizeof berr, cudaMemcpyDeviceToHost, s));
     RM_TRY(take_device_status(s));
     report->backward_error = berr[0];

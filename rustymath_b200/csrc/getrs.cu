@@ -13,15 +13,17 @@
 
 namespace rm {
 
-constexpr int kTB = 64;          // rows of a block row
-constexpr int kKC = 16;          // right-hand-side columns per launch
+constexpr int kTB = kSolveBlock;  // rows of a block row
+constexpr int kKC = kSolveCols;   // right-hand-side columns per launch
 constexpr int kTrsvThreads = 256;
 
-size_t diag_blocks_f64_bytes(int64_t n) { return (size_t)((n + kTB - 1) / kTB) * 2 * kTB * kTB * sizeof(double); }
+size_t diag_blocks_f64_bytes(int64_t n) { return diag_blocks_bytes_max(n); }
 
 // dinv[b][0] = inverse of the lower diagonal block b, dinv[b][1] = inverse of the upper
 // diagonal block b (row-major kTB x kTB; rows/columns past n are identity). A unit triangle
-// takes its diagonal as 1 without reading it.
+// takes its diagonal as 1 without reading it. The triangles are those of the n x n matrix
+// T whose item (i, j) is w[i*ldw + j], or w[j*ldw + i] when COLMAJOR.
+template <bool COLMAJOR>
 __global__ void __launch_bounds__(128) invert_diag_blocks_kernel(const double* __restrict__ w, int64_t ldw, int64_t n,
                                                                  double* __restrict__ dinv, bool lower_unit,
                                                                  bool upper_unit) {
@@ -31,7 +33,10 @@ __global__ void __launch_bounds__(128) invert_diag_blocks_kernel(const double* _
   const int rows = (int)(n - r0 < kTB ? n - r0 : kTB);
   const double* blk = w + r0 * ldw + r0;
   const int col = threadIdx.x;  // threads 0..63 each own one column of the inverse
-  auto A = [&](int i, int j) -> double { return (i < rows && j < rows) ? blk[(int64_t)i * ldw + j] : (i == j ? 1.0 : 0.0); };
+  auto A = [&](int i, int j) -> double {
+    if (i >= rows || j >= rows) return i == j ? 1.0 : 0.0;
+    return COLMAJOR ? blk[(int64_t)j * ldw + i] : blk[(int64_t)i * ldw + j];
+  };
   if (col < kTB) {
     if (which == 0) {
       // lower: x_i = (delta_i,col - sum_{col<=k<i} L_ik x_k) / L_ii for i >= col
@@ -56,11 +61,14 @@ __global__ void __launch_bounds__(128) invert_diag_blocks_kernel(const double* _
   for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) out[e] = x[e / kTB][e % kTB];
 }
 
-int invert_diag_blocks_f64(const double* w, int64_t ldw, int64_t n, double* dinv, bool lower_unit, bool upper_unit,
-                           cudaStream_t stream) {
+int invert_diag_blocks_f64(const double* w, int64_t ldw, bool colmajor, int64_t n, double* dinv, bool lower_unit,
+                           bool upper_unit, cudaStream_t stream) {
   if (n == 0) return RM_OK;
   dim3 grid((unsigned)((n + kTB - 1) / kTB), 2);
-  invert_diag_blocks_kernel<<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
+  if (colmajor)
+    invert_diag_blocks_kernel<true><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
+  else
+    invert_diag_blocks_kernel<false><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
   RM_LAUNCHED();
   return RM_OK;
 }
@@ -74,10 +82,11 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Solves T x = y for kc <= kKC columns of y (in place in x), T the unit lower (LOWER) or
-// upper triangle of the row-major W. flags[nblk] and counter start at zero. Each thread
-// keeps kTB*kKC/kTrsvThreads of its block's running sums in registers.
-template <bool LOWER>
+// Solves T x = y for kc <= kKC columns of y (in place in x), T the lower (LOWER) or upper
+// triangle of the matrix whose item (i, j) is w[i*ldw + j] (w[j*ldw + i] when COLMAJOR);
+// the diagonal blocks' inverses come from dinv. flags[nblk] and counter start at zero.
+// Each thread keeps kTB*kKC/kTrsvThreads of its block's running sums in registers.
+template <bool LOWER, bool COLMAJOR>
 __global__ void __launch_bounds__(kTrsvThreads)
     trsv_chain_kernel(const double* __restrict__ w, int64_t ldw, int n, const double* __restrict__ dinv, double* x,
                       int64_t ldx, int kc, int* flags, int* counter, unsigned* status) {
@@ -105,8 +114,13 @@ __global__ void __launch_bounds__(kTrsvThreads)
     const int c0 = j * kTB, cols = min(kTB, n - c0);
     __syncthreads();  // the previous step's reads of lblk / xs are done
     for (int e = tid; e < kTB * kTB; e += kTrsvThreads) {
-      const int r = e / kTB, c = e % kTB;
-      lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(r0 + r) * ldw + c0 + c] : 0.0;
+      if (COLMAJOR) {  // coalesced along the stored column
+        const int c = e / kTB, r = e % kTB;
+        lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(c0 + c) * ldw + r0 + r] : 0.0;
+      } else {
+        const int r = e / kTB, c = e % kTB;
+        lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(r0 + r) * ldw + c0 + c] : 0.0;
+      }
     }
     if (tid == 0) {
       bool seen = ld_acquire(&flags[j]) != 0;
@@ -182,21 +196,19 @@ __global__ void permute_rows_kernel(const double* __restrict__ b, int64_t ldb, c
   }
 }
 
-size_t getrs_f64_scratch_bytes(int64_t n, int64_t k) {
-  const int64_t nblk = (n + kTB - 1) / kTB;
-  return (size_t)(2 * (nblk + 1)) * sizeof(int) * (size_t)((k + kKC - 1) / kKC + 1) + (size_t)n * k * sizeof(double) +
-         256;
-}
+size_t getrs_f64_scratch_bytes(int64_t n, int64_t k) { return getrs_scratch_bytes_max(n, k); }
 
-int getrs_f64(const double* w, int64_t ldw, int64_t n, const int64_t* perm, const double* dinv, const double* b,
-              int64_t ldb, int64_t k, double* x, int64_t ldx, void* scratch, unsigned* status, cudaStream_t stream,
-              bool trans) {
+int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const int64_t* perm, const double* dinv,
+              const double* b, int64_t ldb, int64_t k, double* x, int64_t ldx, void* scratch, unsigned* status,
+              cudaStream_t stream, bool trans) {
   if (n == 0 || k == 0) return RM_OK;
   const int nblk = (int)((n + kTB - 1) / kTB);
   const int chunks = (int)((k + kKC - 1) / kKC);
-  // b may alias x: gather into a temporary first
+  // The solved triangle pair: L\U itself, or its transpose for A^T x = b.
+  const bool colmajor = trans ? !lu_colmajor : lu_colmajor;
+  // b may alias x: the permuted right-hand side goes to a temporary first
   double* tmp = reinterpret_cast<double*>(scratch);
-  int* flags = reinterpret_cast<int*>(tmp + n * k);
+  int* flags = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + ((size_t)n * k * sizeof(double) + 255) / 256 * 256);
   const size_t flag_bytes = (size_t)(2 * (nblk + 1)) * sizeof(int) * (size_t)chunks;
   RM_CUDA_TRY(cudaMemsetAsync(flags, 0, flag_bytes, stream));
   const int blocks = (int)std::min<int64_t>((n * k + 255) / 256, 4 * device_sm_count());
@@ -205,12 +217,22 @@ int getrs_f64(const double* w, int64_t ldw, int64_t n, const int64_t* perm, cons
   for (int ch = 0; ch < chunks; ++ch) {
     const int kc = (int)std::min<int64_t>(kKC, k - (int64_t)ch * kKC);
     int* f = flags + (size_t)ch * 2 * (nblk + 1);
-    trsv_chain_kernel<true><<<nblk, kTrsvThreads, 0, stream>>>(w, ldw, (int)n, dinv, tmp + ch * kKC, k, kc, f, f + nblk,
-                                                                status);
-    RM_LAUNCHED();
-    trsv_chain_kernel<false><<<nblk, kTrsvThreads, 0, stream>>>(w, ldw, (int)n, dinv, tmp + ch * kKC, k, kc,
-                                                                 f + nblk + 1, f + 2 * nblk + 1, status);
-    RM_LAUNCHED();
+    double* xc = tmp + ch * kKC;
+    if (colmajor) {
+      trsv_chain_kernel<true, true><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f, f + nblk,
+                                                                        status);
+      RM_LAUNCHED();
+      trsv_chain_kernel<false, true><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f + nblk + 1,
+                                                                         f + 2 * nblk + 1, status);
+      RM_LAUNCHED();
+    } else {
+      trsv_chain_kernel<true, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f, f + nblk,
+                                                                         status);
+      RM_LAUNCHED();
+      trsv_chain_kernel<false, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc,
+                                                                          f + nblk + 1, f + 2 * nblk + 1, status);
+      RM_LAUNCHED();
+    }
   }
   permute_rows_kernel<true><<<blocks, 256, 0, stream>>>(tmp, k, trans ? perm : nullptr, n, k, x, ldx, status);
   RM_LAUNCHED();

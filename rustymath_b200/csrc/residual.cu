@@ -10,113 +10,158 @@
 namespace rm {
 
 constexpr int kResWarps = 8;
+constexpr int kResRowsPerWarp = 4;
+constexpr int kResChunk = 256;  // rows of x staged in shared memory at a time
+constexpr int kNormGroup = 16;  // columns per group of norm slots
+constexpr int kNormSlots = 1 + 3 * kNormGroup;
 
-// r (n x k, ldr) = b - A x; rowabs[i] = sum_j |a_ij| (when not NULL). K_MAX >= k.
-template <int K_MAX>
+__device__ __forceinline__ void atomic_max_nonneg(double* p, double v) {
+  // non-negative doubles (and NaN, above +inf) order like their bit patterns
+  if (v > 0.0 || v != v) atomicMax(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));
+}
+
+// r (n x k, ldr) = b - A x, for k <= KC. Each warp owns kResRowsPerWarp rows of A and
+// streams them once; x is staged through shared memory kResChunk rows at a time (every
+// block reads it from L2). norms (zeroed by the caller) collects by atomic maxima
+// norms[0] = ||A||_inf and, per column c, norms[1+c] = ||r_c||_inf (NaN if a residual is
+// NaN) and norms[1+2*kNormGroup+c] = ||b_c||_inf.
+template <int KC>
 __global__ void __launch_bounds__(kResWarps * 32)
     residual_kernel(const double* __restrict__ a, int64_t lda, int64_t n, const double* __restrict__ x, int64_t ldx,
                     const double* __restrict__ b, int64_t ldb, int k, double* __restrict__ r, int64_t ldr,
-                    double* __restrict__ rowabs) {
-  const int lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * kResWarps + (threadIdx.x >> 5);
-  if (row >= n) return;
-  const double* ar = a + row * lda;
-  double s[K_MAX];
+                    double* __restrict__ norms) {
+  __shared__ double xs[KC][kResChunk];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t row0 = ((int64_t)blockIdx.x * kResWarps + warp) * kResRowsPerWarp;
+  double s[kResRowsPerWarp][KC];
+  double absum[kResRowsPerWarp];
 #pragma unroll
-  for (int c = 0; c < K_MAX; ++c) s[c] = 0.0;
-  double abs_sum = 0.0;
-  for (int64_t j = lane; j < n; j += 32) {
-    const double v = __ldcs(ar + j);  // streamed once: keep it out of L2's way
-    abs_sum += fabs(v);
-    const double* xj = x + j * ldx;
+  for (int q = 0; q < kResRowsPerWarp; ++q) {
+    absum[q] = 0.0;
 #pragma unroll
-    for (int c = 0; c < K_MAX; ++c)
-      if (c < k) s[c] = fma(v, __ldg(xj + c), s[c]);
+    for (int c = 0; c < KC; ++c) s[q][c] = 0.0;
+  }
+  for (int64_t j0 = 0; j0 < n; j0 += kResChunk) {
+    __syncthreads();
+    for (int e = tid; e < KC * kResChunk; e += kResWarps * 32) {
+      const int c = e / kResChunk, jj = e % kResChunk;
+      xs[c][jj] = (j0 + jj < n && c < k) ? x[(j0 + jj) * ldx + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kResRowsPerWarp; ++q) {
+      const int64_t row = row0 + q;
+      if (row < n) {
+        const double* ar = a + row * lda + j0;
+        for (int jj = lane; jj < kResChunk && j0 + jj < n; jj += 32) {
+          const double v = __ldcs(ar + jj);  // A streams through once
+          absum[q] += fabs(v);
+#pragma unroll
+          for (int c = 0; c < KC; ++c) s[q][c] = fma(v, xs[c][jj], s[q][c]);
+        }
+      }
+    }
   }
 #pragma unroll
-  for (int off = 16; off; off >>= 1) {
-    abs_sum += __shfl_xor_sync(0xffffffffu, abs_sum, off);
+  for (int q = 0; q < kResRowsPerWarp; ++q) {
 #pragma unroll
-    for (int c = 0; c < K_MAX; ++c) s[c] += __shfl_xor_sync(0xffffffffu, s[c], off);
-  }
-  if (lane < k) {
-    double mine = 0.0;
+    for (int off = 16; off; off >>= 1) {
+      absum[q] += __shfl_xor_sync(0xffffffffu, absum[q], off);
 #pragma unroll
-    for (int c = 0; c < K_MAX; ++c)
-      if (c == lane) mine = s[c];
-    r[row * ldr + lane] = b[row * ldb + lane] - mine;
+      for (int c = 0; c < KC; ++c) s[q][c] += __shfl_xor_sync(0xffffffffu, s[q][c], off);
+    }
+    const int64_t row = row0 + q;
+    if (row < n) {
+      if (lane < k) {
+        double mine = 0.0;
+#pragma unroll
+        for (int c = 0; c < KC; ++c)
+          if (c == lane) mine = s[q][c];
+        const double bv = b[row * ldb + lane];
+        const double rv = bv - mine;
+        r[row * ldr + lane] = rv;
+        if (norms) {
+          atomic_max_nonneg(&norms[1 + lane], fabs(rv));
+          atomic_max_nonneg(&norms[1 + 2 * kNormGroup + lane], fabs(bv));
+        }
+      }
+      if (lane == 0 && norms) atomic_max_nonneg(&norms[0], absum[q]);
+    }
   }
-  if (lane == 0 && rowabs) rowabs[row] = abs_sum;
 }
 
-// norms[0] = max_i rowabs[i]; for each column c: norms[1+3c..] = ||r_c||, ||x_c||, ||b_c||
-// (infinity norms); berr_out[0] = max_c ||r_c|| / (||A|| ||x_c|| + ||b_c||).
-__global__ void __launch_bounds__(1024) backward_error_kernel(const double* __restrict__ rowabs, int64_t n,
-                                                              const double* __restrict__ r, int64_t ldr,
-                                                              const double* __restrict__ x, int64_t ldx,
-                                                              const double* __restrict__ b, int64_t ldb, int k,
-                                                              double* __restrict__ out) {
-  __shared__ double red[32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  auto block_max = [&](double v) -> double {
+// norms[1+kNormGroup+c] = ||x_c||_inf for the n x k (k <= kNormGroup) row-major x.
+__global__ void column_max_kernel(const double* __restrict__ x, int64_t ldx, int64_t n, int k, double* norms) {
+  double m[kNormGroup];
+#pragma unroll
+  for (int c = 0; c < kNormGroup; ++c) m[c] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int c = 0; c < kNormGroup; ++c)
+      if (c < k) m[c] = fmax(m[c], fabs(x[i * ldx + c]));
+#pragma unroll
+  for (int c = 0; c < kNormGroup; ++c) {
+    double v = m[c];
 #pragma unroll
     for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
-#pragma unroll
-    for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
-    return v;
-  };
-  double amax = 0.0;
-  for (int64_t i = tid; i < n; i += blockDim.x) amax = fmax(amax, rowabs[i]);
-  amax = block_max(amax);
+    if ((threadIdx.x & 31) == 0 && c < k) atomic_max_nonneg(&norms[1 + kNormGroup + c], v);
+  }
+}
+
+// out[0] = max_c ||r_c|| / (||A|| ||x_c|| + ||b_c||) over every group of columns (NaN when a
+// residual is NaN), out[1] = ||A||_inf.
+__global__ void backward_error_kernel(const double* __restrict__ norms, int k, double* out) {
+  if (threadIdx.x != 0) return;
+  const double anorm = norms[0];
   double worst = 0.0;
   bool nan = false;
   for (int c = 0; c < k; ++c) {
-    double rn = 0.0, xn = 0.0, bn = 0.0;
-    for (int64_t i = tid; i < n; i += blockDim.x) {
-      const double rv = fabs(r[i * ldr + c]);
-      nan |= rv != rv;
-      rn = fmax(rn, rv);
-      xn = fmax(xn, fabs(x[i * ldx + c]));
-      bn = fmax(bn, fabs(b[i * ldb + c]));
-    }
-    rn = block_max(rn);
-    xn = block_max(xn);
-    bn = block_max(bn);
-    const double den = amax * xn + bn;
-    const double e = den > 0.0 ? rn / den : rn;
-    worst = fmax(worst, e);
+    const double* g = norms + (c / kNormGroup) * kNormSlots;
+    const int cc = c % kNormGroup;
+    const double rn = g[1 + cc], xn = g[1 + kNormGroup + cc], bn = g[1 + 2 * kNormGroup + cc];
+    nan |= rn != rn;
+    const double den = anorm * xn + bn;
+    worst = fmax(worst, den > 0.0 ? rn / den : rn);
   }
-  nan = __syncthreads_or(nan);
-  if (tid == 0) {
-    out[0] = nan ? __longlong_as_double(0x7ff8000000000000ll) : worst;
-    out[1] = amax;
-  }
+  out[0] = nan ? __longlong_as_double(0x7ff8000000000000ll) : worst;
+  out[1] = anorm;
 }
 
+size_t residual_norms_bytes(int64_t k) { return (size_t)((k + kNormGroup - 1) / kNormGroup) * kNormSlots * 8 + 64; }
+
 int residual_f64(const double* a, int64_t lda, int64_t n, const double* x, int64_t ldx, const double* b, int64_t ldb,
-                 int64_t k, double* r, int64_t ldr, double* rowabs, cudaStream_t stream) {
+                 int64_t k, double* r, int64_t ldr, double* norms, cudaStream_t stream) {
   if (n == 0 || k == 0) return RM_OK;
-  const unsigned blocks = (unsigned)((n + kResWarps - 1) / kResWarps);
-  for (int64_t c0 = 0; c0 < k; c0 += 16) {
-    const int kc = (int)std::min<int64_t>(16, k - c0);
+  const int64_t per_block = (int64_t)kResWarps * kResRowsPerWarp;
+  const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
+  if (norms) RM_CUDA_TRY(cudaMemsetAsync(norms, 0, residual_norms_bytes(k), stream));
+  for (int64_t c0 = 0, g = 0; c0 < k; c0 += kNormGroup, ++g) {
+    const int kc = (int)std::min<int64_t>(kNormGroup, k - c0);
+    double* ng = norms ? norms + g * kNormSlots : nullptr;
     if (kc <= 4)
       residual_kernel<4><<<blocks, kResWarps * 32, 0, stream>>>(a, lda, n, x + c0, ldx, b + c0, ldb, kc, r + c0, ldr,
-                                                                 c0 == 0 ? rowabs : nullptr);
+                                                                 ng);
     else
       residual_kernel<16><<<blocks, kResWarps * 32, 0, stream>>>(a, lda, n, x + c0, ldx, b + c0, ldb, kc, r + c0, ldr,
-                                                                  c0 == 0 ? rowabs : nullptr);
+                                                                  ng);
     RM_LAUNCHED();
   }
   return RM_OK;
 }
 
-int backward_error_f64(const double* rowabs, int64_t n, const double* r, int64_t ldr, const double* x, int64_t ldx,
-                       const double* b, int64_t ldb, int64_t k, double* out, cudaStream_t stream) {
-  backward_error_kernel<<<1, 1024, 0, stream>>>(rowabs, n, r, ldr, x, ldx, b, ldb, (int)k, out);
+int backward_error_f64(const double* x, int64_t ldx, int64_t n, int64_t k, double* norms, double* out,
+                       cudaStream_t stream) {
+  if (n == 0 || k == 0) {
+    RM_CUDA_TRY(cudaMemsetAsync(out, 0, 2 * sizeof(double), stream));
+    return RM_OK;
+  }
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, 2 * device_sm_count());
+  for (int64_t c0 = 0, g = 0; c0 < k; c0 += kNormGroup, ++g) {
+    const int kc = (int)std::min<int64_t>(kNormGroup, k - c0);
+    column_max_kernel<<<blocks, 256, 0, stream>>>(x + c0, ldx, n, kc, norms + g * kNormSlots);
+    RM_LAUNCHED();
+  }
+  backward_error_kernel<<<1, 32, 0, stream>>>(norms, (int)k, out);
   RM_LAUNCHED();
   return RM_OK;
 }

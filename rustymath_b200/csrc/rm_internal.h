@@ -35,26 +35,48 @@ int regular_flag_f64(const double* w, int64_t ldw, int64_t n, const double* amax
                      cudaStream_t stream);
 
 // ---------------------------------------------------------------- solves (getrs.cu)
+constexpr int kSolveBlock = 64;  // rows of a block row of the triangular solves
+constexpr int kSolveCols = 16;   // right-hand-side columns per solve launch
+constexpr size_t diag_blocks_bytes_max(int64_t n) {
+  return (size_t)((n + kSolveBlock - 1) / kSolveBlock) * 2 * kSolveBlock * kSolveBlock * sizeof(double);
+}
+constexpr size_t getrs_scratch_bytes_max(int64_t n, int64_t k) {
+  return ((size_t)n * k * sizeof(double) + 255) / 256 * 256 +
+         (size_t)(2 * ((n + kSolveBlock - 1) / kSolveBlock + 1)) * sizeof(int) *
+             (size_t)((k + kSolveCols - 1) / kSolveCols) +
+         256;
+}
 size_t getrs_f64_scratch_bytes(int64_t n, int64_t k);
-// trans == false: x = (P^T L U)^-1 b, w the row-major L\U (W after getrf_f64).
-// trans == true : x = (P^T L U)^-T b, w the row-major transpose of L\U (the column-major
-//                 factors read row by row).
-// b, x row-major n x k (may alias). `dinv` holds the inverted diagonal blocks of w's two
-// triangles from invert_diag_blocks_f64(w, ..., lower_unit = !trans, upper_unit = trans).
-int getrs_f64(const double* w, int64_t ldw, int64_t n, const int64_t* perm, const double* dinv, const double* b,
-              int64_t ldb, int64_t k, double* x, int64_t ldx, void* scratch, unsigned* status, cudaStream_t stream,
-              bool trans = false);
+// x = (P^T L U)^-1 b, or (P^T L U)^-T b when trans, from L\U held row-major in lu (as W
+// after getrf_f64; lu_colmajor false) or column-major (rustymath's factors; lu_colmajor
+// true), with leading dimension ld. b, x row-major n x k (may alias). `dinv` holds the
+// inverted diagonal blocks from invert_diag_blocks_f64 with the arguments that
+// diag_block_args gives for the same (trans, lu_colmajor).
+int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const int64_t* perm, const double* dinv,
+              const double* b, int64_t ldb, int64_t k, double* x, int64_t ldx, void* scratch, unsigned* status,
+              cudaStream_t stream, bool trans = false);
 size_t diag_blocks_f64_bytes(int64_t n);
-int invert_diag_blocks_f64(const double* w, int64_t ldw, int64_t n, double* dinv, bool lower_unit, bool upper_unit,
-                           cudaStream_t stream);
+// Inverts the diagonal blocks of the lower and upper triangles of T, T(i,j) = w[i*ldw+j]
+// (w[j*ldw+i] when colmajor), a unit triangle's diagonal taken as 1.
+int invert_diag_blocks_f64(const double* w, int64_t ldw, bool colmajor, int64_t n, double* dinv, bool lower_unit,
+                           bool upper_unit, cudaStream_t stream);
+struct DiagBlockArgs {
+  bool colmajor, lower_unit, upper_unit;
+};
+inline DiagBlockArgs diag_block_args(bool trans, bool lu_colmajor) {
+  return {trans ? !lu_colmajor : lu_colmajor, !trans, trans};
+}
 
 // ---------------------------------------------------------------- residual (residual.cu)
-// r = b - A x (FP64); rowabs[i] = sum_j |a_ij| when rowabs is not NULL.
+// r = b - A x (FP64). When norms is not NULL (residual_norms_bytes(k) bytes) it also gathers
+// ||A||_inf and the columns' ||r||_inf and ||b||_inf, which backward_error_f64 completes.
+size_t residual_norms_bytes(int64_t k);
 int residual_f64(const double* a, int64_t lda, int64_t n, const double* x, int64_t ldx, const double* b, int64_t ldb,
-                 int64_t k, double* r, int64_t ldr, double* rowabs, cudaStream_t stream);
-// out[0] = normwise backward error (max over columns), out[1] = ||A||_inf.
-int backward_error_f64(const double* rowabs, int64_t n, const double* r, int64_t ldr, const double* x, int64_t ldx,
-                       const double* b, int64_t ldb, int64_t k, double* out, cudaStream_t stream);
+                 int64_t k, double* r, int64_t ldr, double* norms, cudaStream_t stream);
+// After residual_f64 filled norms: out[0] = normwise backward error (max over columns of
+// ||r_c|| / (||A|| ||x_c|| + ||b_c||)), out[1] = ||A||_inf.
+int backward_error_f64(const double* x, int64_t ldx, int64_t n, int64_t k, double* norms, double* out,
+                       cudaStream_t stream);
 
 // dst[j*ldd + i] = src[i*lds + j] for an m x n row-major src.
 int transpose_f64(const double* src, int64_t lds, int64_t m, int64_t n, double* dst, int64_t ldd, cudaStream_t stream);

@@ -254,3 +254,17 @@ def test_device_tensors(rb):
     assert np.array_equal(fac.p.cpu().numpy(), po)
     c = rb.matmul(ta, tb)
     assert np.allclose(c.cpu().numpy(), a @ b, rtol=1e-13, atol=1e-12)
+
+
+@pytest.mark.parametrize("k", [1, 5, 16, 17, 40])
+def test_backward_error_report(rb, k):
+    """The device's FP64 backward error agrees with the oracle's double-double one."""
+    n = 700
+    rng = np.random.default_rng(k)
+    a = rng.standard_normal((n, n)) + np.sqrt(n) * np.eye(n)
+    b = rng.standard_normal((n, k))
+    x, reps = rb.solve_report(a, b)
+    want = O.backward_error(a, x, b)
+    got = reps[0].backward_error
+    assert got <= n * 2.0 ** -53 and want <= n * 2.0 ** -53
+    assert abs(got - want) <= 4 * EPS * max(1.0, np.sqrt(n)) + 0.5 * want
