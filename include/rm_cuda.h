@@ -102,6 +102,20 @@ int rm_dlu_solve(int64_t n, const double *d_factors, const int64_t *d_perm, cons
 int rm_dlu_solve_host(int64_t n, const double *h_factors, const int64_t *h_perm,
                       const double *h_b, int64_t k, double *h_x, int trans);
 
+/* rm_dlu_solve for callers that cannot allocate device memory during a call (a fixed
+ * memory budget or arena that owns all device memory, a real-time loop kept away from the
+ * allocator). It has no counterpart in the reference. Its scratch is a fixed __device__
+ * array inside the library (about 4.7 MB, held on every GPU that loads the library until
+ * the process exits), so it takes n <= RM_NOALLOC_MAX_N and k <= RM_NOALLOC_MAX_K and
+ * returns RM_BAD_ARG beyond them. The first call on a device looks the array up (once per
+ * device); make that first call before any stream capture. All calls on one GPU share that
+ * GPU's array and each leaves its contents for the next: calls that overlap on the same
+ * GPU (on different streams) race on it, so the caller serialises them. */
+#define RM_NOALLOC_MAX_N 4096
+#define RM_NOALLOC_MAX_K 16
+int rm_dlu_solve_noalloc(int64_t n, const double *d_factors, const int64_t *d_perm,
+                         const double *d_b, int64_t k, double *d_x, int trans, void *stream);
+
 /* x = A^-1 b for the n x n row-major A and n x k row-major b, by the method in opts (NULL:
  * plain float64). Returns RM_NOT_REGULAR, writing nothing to x, where rustymath's solve
  * would take its least-squares route (factor.rs:207-209). Synchronises on `stream`. */

@@ -40,6 +40,7 @@ SIGNATURES = {
     "rm_dlu_factor_host": (ctypes.c_int, [_i64, _p, _p, _p, ctypes.POINTER(_i32)]),
     "rm_dlu_solve": (ctypes.c_int, [_i64, _p, _p, _p, _i64, _p, ctypes.c_int, _p]),
     "rm_dlu_solve_host": (ctypes.c_int, [_i64, _p, _p, _p, _i64, _p, ctypes.c_int]),
+    "rm_dlu_solve_noalloc": (ctypes.c_int, [_i64, _p, _p, _p, _i64, _p, ctypes.c_int, _p]),
     "rm_dsolve": (ctypes.c_int, [_i64, _p, _p, _i64, _p, ctypes.POINTER(SolveOptions), ctypes.POINTER(SolveReport),
                                  _p]),
     "rm_dsolve_host": (ctypes.c_int, [_i64, _p, _p, _i64, _p, ctypes.POINTER(SolveOptions),
