@@ -381,6 +381,48 @@ int rm_dgemm_host(int transa, int transb, int64_t m, int64_t n, int64_t k, doubl
   return st;
 }
 
+int rm_sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* d_a, int64_t lda,
+                const float* d_b, int64_t ldb, float beta, float* d_c, int64_t ldc, void* stream) {
+  if (m < 0 || n < 0 || k < 0 || (passes != 1 && passes != 3)) return RM_BAD_ARG;
+  if (m == 0 || n == 0) return RM_OK;
+  if (ldc < n || (k > 0 && (lda < k || ldb < k)) || !d_c || (k > 0 && (!d_a || !d_b))) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  if (k == 0 || alpha == 0.0f) return scale_f32(d_c, ldc, m, n, beta, s);
+  // operands go to 16-byte aligned, padded copies when needed; the low parts always do
+  const bool fix_a = (reinterpret_cast<uintptr_t>(d_a) & 15) || (lda & 3);
+  const bool fix_b = (reinterpret_cast<uintptr_t>(d_b) & 15) || (ldb & 3);
+  const int64_t pk = round_up(k, 4);
+  Arena ar;
+  const size_t oa = fix_a ? ar.add((size_t)m * pk * 4) : 0, ob = fix_b ? ar.add((size_t)n * pk * 4) : 0;
+  const size_t oal = passes == 3 ? ar.add((size_t)m * pk * 4) : 0, obl = passes == 3 ? ar.add((size_t)n * pk * 4) : 0;
+  Scratch sc;
+  sc.stream = s;
+  if (ar.total) RM_TRY(scratch_alloc(&sc.base, ar.total, s));
+  const float* a = d_a;
+  const float* b = d_b;
+  int64_t la = lda, lb = ldb;
+  if (fix_a) {
+    RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<float>(oa), pk * 4, d_a, lda * 4, k * 4, m, cudaMemcpyDeviceToDevice, s));
+    a = sc.at<float>(oa);
+    la = pk;
+  }
+  if (fix_b) {
+    RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<float>(ob), pk * 4, d_b, ldb * 4, k * 4, n, cudaMemcpyDeviceToDevice, s));
+    b = sc.at<float>(ob);
+    lb = pk;
+  }
+  const float* alo = nullptr;
+  const float* blo = nullptr;
+  if (passes == 3) {
+    RM_TRY(split_lo_f32(a, la, m, k, sc.at<float>(oal), pk, s));
+    RM_TRY(split_lo_f32(b, lb, n, k, sc.at<float>(obl), pk, s));
+    alo = sc.at<float>(oal);
+    blo = sc.at<float>(obl);
+  }
+  return sgemm_tc(passes, m, n, k, alpha, a, la, alo, pk, b, lb, blo, pk, beta, d_c, ldc, device_status(), s);
+}
+
 int rm_dlu_factor(int64_t n, const double* d_a, double* d_factors, int64_t* d_perm, int32_t* h_regular, void* stream) {
   if (n < 0 || (n > 0 && (!d_a || !d_factors || !d_perm))) return RM_BAD_ARG;
   if (h_regular) *h_regular = 0;

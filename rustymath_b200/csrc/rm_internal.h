@@ -16,6 +16,16 @@ int dgemm_device(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha
                  cudaStream_t stream, bool force_wide_m = false);
 int scale_device(double* c, int64_t ldc, int64_t m, int64_t n, double beta, cudaStream_t stream);
 
+// ---------------------------------------------------------------- FP32 tensor-core GEMM (sgemm_tc.cu)
+// C = alpha A B^T + beta C, A m x k and B n x k K-major (lda, ldb % 4 == 0, 16-byte bases),
+// C row-major. passes 1: TF32 inputs; passes 3: alo/blo hold x - trunc_tf32(x) and three
+// products give float32-level accuracy.
+int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* alo,
+             int64_t ldalo, const float* b, int64_t ldb, const float* blo, int64_t ldblo, float beta, float* c,
+             int64_t ldc, unsigned* status, cudaStream_t stream);
+int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStream_t stream);
+int split_lo_f32(const float* x, int64_t ldx, int64_t m, int64_t k, float* lo, int64_t ldl, cudaStream_t stream);
+
 // ---------------------------------------------------------------- LU (getrf.cu)
 // Row-major working matrix W (n rows, ldw >= n, ldw % 32 == 0, 16-byte aligned). On return
 // W holds L\U of P*A row by row, ipiv[c] is the row swapped with row c (absolute) and
