@@ -61,6 +61,14 @@ def make_system(n, nrhs, seed, device):
     return a.contiguous(), b.contiguous()
 
 
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
@@ -204,36 +212,49 @@ def main():
     n, k = args.n, args.nrhs
     a, b = make_system(n, k, rank, dev)
     x = torch.empty_like(b)
-    method = args.method if args.method != "auto" else "plain"
-    opts = rb.linalg._options(method)
-    rep = _lib.SolveReport()
+    method = args.method if args.method != "auto" else "mixed"
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
 
-    def step():
-        st = lib.rm_dsolve(n, a.data_ptr(), b.data_ptr(), k, x.data_ptr(), ctypes.byref(opts), ctypes.byref(rep), sp)
-        _lib.check(st, "rm_dsolve")
+    def timed(meth, steps, warmup, clocks=None):
+        """(seconds for `steps` solves, max over ranks; report; launches per solve)"""
+        opts = rb.linalg._options(meth)
+        rep = _lib.SolveReport()
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    launches0 = lib.rm_launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(args.steps):
+        def step():
+            st = lib.rm_dsolve(n, a.data_ptr(), b.data_ptr(), k, x.data_ptr(), ctypes.byref(opts), ctypes.byref(rep),
+                               sp)
+            _lib.check(st, "rm_dsolve")
+
+        for _ in range(warmup):
             step()
-        e1.record()
         torch.cuda.synchronize()
-    launches = (lib.rm_launch_count() - launches0) // max(args.steps, 1)
-    elapsed = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+        if world > 1:
+            dist.barrier()
+        launches0 = lib.rm_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with (clocks if clocks is not None else _Null()):
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(steps):
+                step()
+            e1.record()
+            torch.cuda.synchronize()
+        launches = (lib.rm_launch_count() - launches0) // max(steps, 1)
+        elapsed = e0.elapsed_time(e1) / 1e3
+        if world > 1:
+            t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            elapsed = float(t.item())
+        return elapsed, rep, launches
+
+    # the plain float64 LU first (the comparison arm), then the headline method
+    plain_t, plain_rep, plain_launches = timed("plain", max(1, min(args.steps, 3)), args.warmup)
+    plain = {"solves_per_s": world * max(1, min(args.steps, 3)) / plain_t,
+             "ms_per_solve": 1e3 * plain_t / max(1, min(args.steps, 3)), "backward_error": plain_rep.backward_error,
+             "gpu_launches": int(plain_launches)}
+    clocks = ClockSampler(local)
+    elapsed, rep, launches = timed(method, args.steps, args.warmup, clocks)
     value = world * args.steps / elapsed
     berr = rep.backward_error
     method_used = "plain FP64 LU" if rep.method_used == _lib.RM_METHOD_PLAIN_F64 else "FP32 LU + FP64 refinement"
@@ -242,7 +263,8 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "n": n, "nrhs": k,
                               "ms_per_step": 1e3 * elapsed / args.steps, "backward_error": rep.backward_error,
-                              "method": method_used, "gpu_launches": int(launches)}), flush=True)
+                              "method": method_used, "gpu_launches": int(launches), "plain_fp64": plain,
+                              "iterations": rep.iterations, "fell_back": rep.fell_back}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -255,6 +277,8 @@ def main():
     b_h.copy_(b)
     an, bn, xn = a_h.numpy(), b_h.numpy(), x_h.numpy()
     e2e_steps = max(1, min(args.steps, 3))
+    opts = rb.linalg._options(method)
+    rep = _lib.SolveReport()
     lib.rm_dsolve_host(n, an.ctypes.data, bn.ctypes.data, k, xn.ctypes.data, ctypes.byref(opts), ctypes.byref(rep))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -277,6 +301,8 @@ def main():
         if not args.no_cpu_baseline:
             cpu, x_cpu = cpu_baseline(a_h.numpy(), b_h.numpy())
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+                "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["solves_per_s"],
+                "refinement_iterations": rep.iterations, "fell_back": rep.fell_back,
                 "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if method == "plain" else "f32+f64",
                 "data": "synthetic",

@@ -85,15 +85,15 @@ int rm_dgemm_host(int transa, int transb, int64_t m, int64_t n, int64_t k, doubl
                   const double *h_a, int64_t lda, const double *h_b, int64_t ldb, double beta,
                   double *h_c, int64_t ldc);
 
-/* C = alpha * A * B^T + beta * C in float32 on the tensor cores (tcgen05, kind::tf32):
- * A is m x k and B is n x k, both row-major with k contiguous; C is m x n row-major.
- * passes = 1 reads the inputs as TF32; passes = 3 splits each operand into a TF32 part and
- * a low part and sums three products, for float32-level accuracy. The building block of
- * the mixed-precision solve; it has no counterpart in rustymath, whose float32 products
- * run on its CPU kernels. */
-int rm_sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float *d_a,
-                int64_t lda, const float *d_b, int64_t ldb, float beta, float *d_c, int64_t ldc,
-                void *stream);
+/* C = alpha * A * op(B) + beta * C in float32 on the tensor cores (tcgen05, kind::tf32):
+ * A is m x k row-major; op(B) = B (k x n row-major) or, with transb = RM_TRANS, B^T (B
+ * n x k row-major); C is m x n row-major. passes = 1 reads the inputs as TF32; passes = 3
+ * splits each operand into a TF32 part and a low part and sums three products, for
+ * float32-level accuracy. The building block of the mixed-precision solve; it has no
+ * counterpart in rustymath, whose float32 products run on its CPU kernels. */
+int rm_sgemm_tc(int passes, int transb, int64_t m, int64_t n, int64_t k, float alpha,
+                const float *d_a, int64_t lda, const float *d_b, int64_t ldb, float beta,
+                float *d_c, int64_t ldc, void *stream);
 
 /* LU with partial pivoting of the n x n row-major d_a into column-major d_factors and
  * d_perm (int64), as lu_factor (core/src/linalg/factor.rs:617-630) gives them. When

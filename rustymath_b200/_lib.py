@@ -36,7 +36,7 @@ SIGNATURES = {
                                 _i64, _p]),
     "rm_dgemm_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _i64, _i64, _f64, _p, _i64, _p, _i64, _f64,
                                      _p, _i64]),
-    "rm_sgemm_tc": (ctypes.c_int, [ctypes.c_int, _i64, _i64, _i64, ctypes.c_float, _p, _i64, _p, _i64,
+    "rm_sgemm_tc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _i64, _i64, ctypes.c_float, _p, _i64, _p, _i64,
                                    ctypes.c_float, _p, _i64, _p]),
     "rm_dlu_factor": (ctypes.c_int, [_i64, _p, _p, _p, ctypes.POINTER(_i32), _p]),
     "rm_dlu_factor_host": (ctypes.c_int, [_i64, _p, _p, _p, ctypes.POINTER(_i32)]),

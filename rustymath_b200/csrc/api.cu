@@ -381,21 +381,22 @@ int rm_dgemm_host(int transa, int transb, int64_t m, int64_t n, int64_t k, doubl
   return st;
 }
 
-int rm_sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* d_a, int64_t lda,
+int rm_sgemm_tc(int passes, int transb, int64_t m, int64_t n, int64_t k, float alpha, const float* d_a, int64_t lda,
                 const float* d_b, int64_t ldb, float beta, float* d_c, int64_t ldc, void* stream) {
-  if (m < 0 || n < 0 || k < 0 || (passes != 1 && passes != 3)) return RM_BAD_ARG;
+  if (m < 0 || n < 0 || k < 0 || (passes != 1 && passes != 3) || (transb != 0 && transb != 1)) return RM_BAD_ARG;
   if (m == 0 || n == 0) return RM_OK;
-  if (ldc < n || (k > 0 && (lda < k || ldb < k)) || !d_c || (k > 0 && (!d_a || !d_b))) return RM_BAD_ARG;
+  const int64_t bcols = transb ? k : n;
+  if (ldc < n || (k > 0 && (lda < k || ldb < bcols)) || !d_c || (k > 0 && (!d_a || !d_b))) return RM_BAD_ARG;
   RM_TRY(check_device());
   cudaStream_t s = as_stream(stream);
   if (k == 0 || alpha == 0.0f) return scale_f32(d_c, ldc, m, n, beta, s);
-  // operands go to 16-byte aligned, padded copies when needed; the low parts always do
+  // operands go to 16-byte aligned, padded copies when needed; a k x n B is transposed
+  // into n x k (the tensor cores read both operands with k contiguous)
   const bool fix_a = (reinterpret_cast<uintptr_t>(d_a) & 15) || (lda & 3);
-  const bool fix_b = (reinterpret_cast<uintptr_t>(d_b) & 15) || (ldb & 3);
-  const int64_t pk = round_up(k, 4);
+  const bool fix_b = !transb || (reinterpret_cast<uintptr_t>(d_b) & 15) || (ldb & 3);
+  const int64_t pa = round_up(k, 4), pb = round_up(k, 4);
   Arena ar;
-  const size_t oa = fix_a ? ar.add((size_t)m * pk * 4) : 0, ob = fix_b ? ar.add((size_t)n * pk * 4) : 0;
-  const size_t oal = passes == 3 ? ar.add((size_t)m * pk * 4) : 0, obl = passes == 3 ? ar.add((size_t)n * pk * 4) : 0;
+  const size_t oa = fix_a ? ar.add((size_t)m * pa * 4) : 0, ob = fix_b ? ar.add((size_t)n * pb * 4) : 0;
   Scratch sc;
   sc.stream = s;
   if (ar.total) RM_TRY(scratch_alloc(&sc.base, ar.total, s));
@@ -403,24 +404,20 @@ int rm_sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const 
   const float* b = d_b;
   int64_t la = lda, lb = ldb;
   if (fix_a) {
-    RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<float>(oa), pk * 4, d_a, lda * 4, k * 4, m, cudaMemcpyDeviceToDevice, s));
+    RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<float>(oa), pa * 4, d_a, lda * 4, k * 4, m, cudaMemcpyDeviceToDevice, s));
     a = sc.at<float>(oa);
-    la = pk;
+    la = pa;
   }
   if (fix_b) {
-    RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<float>(ob), pk * 4, d_b, ldb * 4, k * 4, n, cudaMemcpyDeviceToDevice, s));
+    if (transb) {
+      RM_CUDA_TRY(cudaMemcpy2DAsync(sc.at<float>(ob), pb * 4, d_b, ldb * 4, k * 4, n, cudaMemcpyDeviceToDevice, s));
+    } else {
+      RM_TRY(transpose_f32(d_b, ldb, k, n, sc.at<float>(ob), pb, s));
+    }
     b = sc.at<float>(ob);
-    lb = pk;
+    lb = pb;
   }
-  const float* alo = nullptr;
-  const float* blo = nullptr;
-  if (passes == 3) {
-    RM_TRY(split_lo_f32(a, la, m, k, sc.at<float>(oal), pk, s));
-    RM_TRY(split_lo_f32(b, lb, n, k, sc.at<float>(obl), pk, s));
-    alo = sc.at<float>(oal);
-    blo = sc.at<float>(obl);
-  }
-  return sgemm_tc(passes, m, n, k, alpha, a, la, alo, pk, b, lb, blo, pk, beta, d_c, ldc, device_status(), s);
+  return sgemm_tc(passes, m, n, k, alpha, a, la, b, lb, beta, d_c, ldc, device_status(), s);
 }
 
 int rm_dlu_factor(int64_t n, const double* d_a, double* d_factors, int64_t* d_perm, int32_t* h_regular, void* stream) {
@@ -571,6 +568,87 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   return take_device_status(s);
 }
 
+// The mixed-precision solve: butterflies, unpivoted float32 LU on the tensor cores, float64
+// refinement until the backward error reaches the tolerance; stalls fall back to the plain
+// float64 solve (when opts->fallback) or return RM_NO_CONVERGENCE.
+static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t k, double* d_x,
+                        const rm_solve_options* opts, rm_solve_report* report, cudaStream_t s) {
+  const int64_t N = round_up(n, 4), ldr = round_up(N, 32);
+  const double tol = opts->tolerance > 0.0 ? opts->tolerance : (double)n * 0x1.0p-53;
+  const int max_it = opts->max_iterations > 0 ? opts->max_iterations : 30;
+  int iterations = 0;
+  bool converged = false;
+  double berr_h = 0.0;
+  {
+    Arena ar;
+    const size_t oar = ar.add((size_t)N * ldr * 4), oru = ar.add((size_t)2 * N * 8), orv = ar.add((size_t)2 * N * 8);
+    const size_t olu = ar.add(getrf_genp_f32_scratch_bytes(N)), odinv = ar.add(diag_blocks_f32_bytes(N));
+    const size_t oc = ar.add((size_t)N * k * 4), orr = ar.add((size_t)n * k * 8), onorm = ar.add(residual_norms_bytes(k));
+    const size_t oberr = ar.add(2 * sizeof(double)), otr = ar.add(trsv_f32_scratch_bytes(N, k));
+    Scratch sc;
+    sc.stream = s;
+    RM_TRY(scratch_alloc(&sc.base, ar.total, s));
+    float* arf = sc.at<float>(oar);
+    const double* ru = sc.at<double>(oru);
+    const double* rv = sc.at<double>(orv);
+    float* c = sc.at<float>(oc);
+    unsigned* st = device_status();
+    RM_TRY(butterfly_params(sc.at<double>(oru), N, 0x5eed0001ull, s));
+    RM_TRY(butterfly_params(sc.at<double>(orv), N, 0x5eed0002ull, s));
+    RM_TRY(rbt_matrix(d_a, n, n, N, ru, rv, arf, ldr, s));
+    RM_TRY(getrf_genp_f32(arf, ldr, N, sc.at<void>(olu), st, s));
+    RM_TRY(invert_diag_blocks_f32(arf, ldr, N, sc.at<float>(odinv), s));
+    // x0 = V (LU)^-1 U^T b
+    RM_TRY(rbt_left(d_b, k, n, N, k, ru, c, k, s));
+    RM_TRY(lu_solve_f32_nopiv(arf, ldr, N, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
+    RM_TRY(rbt_right_add(c, k, n, N, k, rv, d_x, k, true, s));
+    double prev = INFINITY;
+    for (int it = 0; it <= max_it; ++it) {
+      RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
+      RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(oberr), s));
+      RM_CUDA_TRY(cudaMemcpyAsync(&berr_h, sc.at<double>(oberr), sizeof berr_h, cudaMemcpyDeviceToHost, s));
+      const int dst = take_device_status(s);  // synchronises
+      if (dst != RM_OK) return dst;
+      if (berr_h <= tol) {
+        converged = true;
+        break;
+      }
+      if (!(berr_h < 0.5 * prev) || it == max_it) break;  // stalled, diverging, NaN, or out of steps
+      prev = berr_h;
+      // x += V (LU)^-1 U^T r
+      RM_TRY(rbt_left(sc.at<double>(orr), k, n, N, k, ru, c, k, s));
+      RM_TRY(lu_solve_f32_nopiv(arf, ldr, N, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
+      RM_TRY(rbt_right_add(c, k, n, N, k, rv, d_x, k, false, s));
+      ++iterations;
+    }
+  }
+  if (converged) {
+    if (report) {
+      report->backward_error = berr_h;
+      report->iterations = iterations;
+      report->method_used = RM_METHOD_F32_IR;
+      report->fell_back = 0;
+      report->regular = 1;
+    }
+    return RM_OK;
+  }
+  if (!opts->fallback) {
+    if (report) {
+      report->backward_error = berr_h;
+      report->iterations = iterations;
+      report->method_used = RM_METHOD_F32_IR;
+    }
+    set_last_message("mixed-precision refinement stalled above the tolerance");
+    return RM_NO_CONVERGENCE;
+  }
+  const int st = dsolve_plain(n, d_a, d_b, k, d_x, report, s);
+  if (report) {
+    report->iterations = iterations;
+    report->fell_back = 1;
+  }
+  return st;
+}
+
 int rm_dsolve(int64_t n, const double* d_a, const double* d_b, int64_t k, double* d_x, const rm_solve_options* opts,
               rm_solve_report* report, void* stream) {
   if (n < 0 || k < 0) return RM_BAD_ARG;
@@ -584,6 +662,8 @@ int rm_dsolve(int64_t n, const double* d_a, const double* d_b, int64_t k, double
   if (method != RM_METHOD_PLAIN_F64 && method != RM_METHOD_F32_IR) return RM_BAD_ARG;
   RM_TRY(check_device());
   cudaStream_t s = as_stream(stream);
+  if (k == 0) return RM_OK;
+  if (method == RM_METHOD_F32_IR) return dsolve_mixed(n, d_a, d_b, k, d_x, opts, report, s);
   return dsolve_plain(n, d_a, d_b, k, d_x, report, s);
 }
 

@@ -23,41 +23,40 @@ size_t diag_blocks_f64_bytes(int64_t n) { return diag_blocks_bytes_max(n); }
 // diagonal block b (row-major kTB x kTB; rows/columns past n are identity). A unit triangle
 // takes its diagonal as 1 without reading it. The triangles are those of the n x n matrix
 // T whose item (i, j) is w[i*ldw + j], or w[j*ldw + i] when COLMAJOR.
-template <bool COLMAJOR>
-__global__ void __launch_bounds__(128) invert_diag_blocks_kernel(const double* __restrict__ w, int64_t ldw, int64_t n,
-                                                                 double* __restrict__ dinv, bool lower_unit,
-                                                                 bool upper_unit) {
-  __shared__ double x[kTB][kTB + 1];
+template <typename T, bool COLMAJOR>
+__global__ void __launch_bounds__(128) invert_diag_blocks_kernel(const T* __restrict__ w, int64_t ldw, int64_t n,
+                                                                 T* __restrict__ dinv, bool lower_unit, bool upper_unit) {
+  __shared__ T x[kTB][kTB + 1];
   const int b = blockIdx.x, which = blockIdx.y;  // 0: L, 1: U
   const int64_t r0 = (int64_t)b * kTB;
   const int rows = (int)(n - r0 < kTB ? n - r0 : kTB);
-  const double* blk = w + r0 * ldw + r0;
+  const T* blk = w + r0 * ldw + r0;
   const int col = threadIdx.x;  // threads 0..63 each own one column of the inverse
-  auto A = [&](int i, int j) -> double {
-    if (i >= rows || j >= rows) return i == j ? 1.0 : 0.0;
+  auto A = [&](int i, int j) -> T {
+    if (i >= rows || j >= rows) return i == j ? T(1) : T(0);
     return COLMAJOR ? blk[(int64_t)j * ldw + i] : blk[(int64_t)i * ldw + j];
   };
   if (col < kTB) {
     if (which == 0) {
       // lower: x_i = (delta_i,col - sum_{col<=k<i} L_ik x_k) / L_ii for i >= col
       for (int i = 0; i < kTB; ++i) {
-        double s = i == col ? 1.0 : 0.0;
+        T s = i == col ? T(1) : T(0);
         if (i > col)
           for (int k = col; k < i; ++k) s = fma(-A(i, k), x[k][col], s);
-        x[i][col] = i < col ? 0.0 : (lower_unit ? s : s / A(i, i));
+        x[i][col] = i < col ? T(0) : (lower_unit ? s : s / A(i, i));
       }
     } else {
       // upper: x_i = (delta_i,col - sum_{i<k<=col} U_ik x_k) / U_ii for i <= col
       for (int i = kTB - 1; i >= 0; --i) {
-        double s = i == col ? 1.0 : 0.0;
+        T s = i == col ? T(1) : T(0);
         if (i < col)
           for (int k = i + 1; k <= col; ++k) s = fma(-A(i, k), x[k][col], s);
-        x[i][col] = i > col ? 0.0 : (upper_unit ? s : s / A(i, i));
+        x[i][col] = i > col ? T(0) : (upper_unit ? s : s / A(i, i));
       }
     }
   }
   __syncthreads();
-  double* out = dinv + ((int64_t)b * 2 + which) * kTB * kTB;
+  T* out = dinv + ((int64_t)b * 2 + which) * kTB * kTB;
   for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) out[e] = x[e / kTB][e % kTB];
 }
 
@@ -66,9 +65,9 @@ int invert_diag_blocks_f64(const double* w, int64_t ldw, bool colmajor, int64_t 
   if (n == 0) return RM_OK;
   dim3 grid((unsigned)((n + kTB - 1) / kTB), 2);
   if (colmajor)
-    invert_diag_blocks_kernel<true><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
+    invert_diag_blocks_kernel<double, true><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
   else
-    invert_diag_blocks_kernel<false><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
+    invert_diag_blocks_kernel<double, false><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
   RM_LAUNCHED();
   return RM_OK;
 }
@@ -86,13 +85,13 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // triangle of the matrix whose item (i, j) is w[i*ldw + j] (w[j*ldw + i] when COLMAJOR);
 // the diagonal blocks' inverses come from dinv. flags[nblk] and counter start at zero.
 // Each thread keeps kTB*kKC/kTrsvThreads of its block's running sums in registers.
-template <bool LOWER, bool COLMAJOR>
+template <typename T, bool LOWER, bool COLMAJOR>
 __global__ void __launch_bounds__(kTrsvThreads)
-    trsv_chain_kernel(const double* __restrict__ w, int64_t ldw, int n, const double* __restrict__ dinv, double* x,
-                      int64_t ldx, int kc, int* flags, int* counter, unsigned* status) {
+    trsv_chain_kernel(const T* __restrict__ w, int64_t ldw, int n, const T* __restrict__ dinv, T* x, int64_t ldx,
+                      int kc, int* flags, int* counter, unsigned* status) {
   constexpr int PER = kTB * kKC / kTrsvThreads;
-  __shared__ double lblk[kTB][kTB];
-  __shared__ double xs[kTB][kKC];
+  __shared__ T lblk[kTB][kTB];
+  __shared__ T xs[kTB][kKC];
   __shared__ int ticket, good;
   const int tid = threadIdx.x;
   const int nblk = (n + kTB - 1) / kTB;
@@ -102,11 +101,11 @@ __global__ void __launch_bounds__(kTrsvThreads)
   const int b = LOWER ? t : nblk - 1 - t;
   const int r0 = b * kTB, rows = min(kTB, n - r0);
 
-  double acc[PER];
+  T acc[PER];
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
     const int e = tid + i * kTrsvThreads, r = e / kKC, c = e % kKC;
-    acc[i] = (r < rows && c < kc) ? x[(int64_t)(r0 + r) * ldx + c] : 0.0;
+    acc[i] = (r < rows && c < kc) ? x[(int64_t)(r0 + r) * ldx + c] : T(0);
   }
   bool ok = true;
   for (int s = 0; s < t; ++s) {
@@ -116,10 +115,10 @@ __global__ void __launch_bounds__(kTrsvThreads)
     for (int e = tid; e < kTB * kTB; e += kTrsvThreads) {
       if (COLMAJOR) {  // coalesced along the stored column
         const int c = e / kTB, r = e % kTB;
-        lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(c0 + c) * ldw + r0 + r] : 0.0;
+        lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(c0 + c) * ldw + r0 + r] : T(0);
       } else {
         const int r = e / kTB, c = e % kTB;
-        lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(r0 + r) * ldw + c0 + c] : 0.0;
+        lblk[r][c] = (r < rows && c < cols) ? w[(int64_t)(r0 + r) * ldw + c0 + c] : T(0);
       }
     }
     if (tid == 0) {
@@ -141,13 +140,13 @@ __global__ void __launch_bounds__(kTrsvThreads)
     }
     for (int e = tid; e < kTB * kKC; e += kTrsvThreads) {
       const int r = e / kKC, c = e % kKC;
-      xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : 0.0;
+      xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : T(0);
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int e = tid + i * kTrsvThreads, r = e / kKC, c = e % kKC;
-      double s2 = acc[i];
+      T s2 = acc[i];
 #pragma unroll 16
       for (int q = 0; q < kTB; ++q) s2 = fma(-lblk[r][q], xs[q][c], s2);
       acc[i] = s2;
@@ -155,7 +154,7 @@ __global__ void __launch_bounds__(kTrsvThreads)
   }
   __syncthreads();
   if (ok) {
-    const double* dv = dinv + ((int64_t)b * 2 + (LOWER ? 0 : 1)) * kTB * kTB;
+    const T* dv = dinv + ((int64_t)b * 2 + (LOWER ? 0 : 1)) * kTB * kTB;
     for (int e = tid; e < kTB * kTB; e += kTrsvThreads) lblk[e / kTB][e % kTB] = dv[e];
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
@@ -166,7 +165,7 @@ __global__ void __launch_bounds__(kTrsvThreads)
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int e = tid + i * kTrsvThreads, r = e / kKC, c = e % kKC;
-      double s2 = 0.0;
+      T s2 = T(0);
 #pragma unroll 16
       for (int q = 0; q < kTB; ++q) s2 = fma(lblk[r][q], xs[q][c], s2);
       if (r < rows && c < kc) x[(int64_t)(r0 + r) * ldx + c] = s2;
@@ -219,23 +218,61 @@ int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const i
     int* f = flags + (size_t)ch * 2 * (nblk + 1);
     double* xc = tmp + ch * kKC;
     if (colmajor) {
-      trsv_chain_kernel<true, true><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f, f + nblk,
-                                                                        status);
+      trsv_chain_kernel<double, true, true><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f,
+                                                                                f + nblk, status);
       RM_LAUNCHED();
-      trsv_chain_kernel<false, true><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f + nblk + 1,
-                                                                         f + 2 * nblk + 1, status);
+      trsv_chain_kernel<double, false, true><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc,
+                                                                                 f + nblk + 1, f + 2 * nblk + 1, status);
       RM_LAUNCHED();
     } else {
-      trsv_chain_kernel<true, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f, f + nblk,
-                                                                         status);
+      trsv_chain_kernel<double, true, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc, f,
+                                                                                 f + nblk, status);
       RM_LAUNCHED();
-      trsv_chain_kernel<false, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc,
-                                                                          f + nblk + 1, f + 2 * nblk + 1, status);
+      trsv_chain_kernel<double, false, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, k, kc,
+                                                                                  f + nblk + 1, f + 2 * nblk + 1, status);
       RM_LAUNCHED();
     }
   }
   permute_rows_kernel<true><<<blocks, 256, 0, stream>>>(tmp, k, trans ? perm : nullptr, n, k, x, ldx, status);
   RM_LAUNCHED();
+  return RM_OK;
+}
+
+// ------------------------------------------------------------------ float32, no pivoting
+
+size_t diag_blocks_f32_bytes(int64_t n) { return diag_blocks_bytes_max(n) / 2; }
+
+int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream) {
+  if (n == 0) return RM_OK;
+  dim3 grid((unsigned)((n + kTB - 1) / kTB), 2);
+  invert_diag_blocks_kernel<float, false><<<grid, 128, 0, stream>>>(w, ldw, n, dinv, true, false);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+size_t trsv_f32_scratch_bytes(int64_t n, int64_t k) {
+  return (size_t)(2 * ((n + kTB - 1) / kTB + 1)) * sizeof(int) * (size_t)((k + kKC - 1) / kKC) + 256;
+}
+
+// x = U^-1 L^-1 x in place for the row-major float32 L\U (unit L) of an unpivoted LU.
+int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, float* x, int64_t ldx, int64_t k,
+                       void* scratch, unsigned* status, cudaStream_t stream) {
+  if (n == 0 || k == 0) return RM_OK;
+  const int nblk = (int)((n + kTB - 1) / kTB);
+  const int chunks = (int)((k + kKC - 1) / kKC);
+  int* flags = reinterpret_cast<int*>(scratch);
+  RM_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)(2 * (nblk + 1)) * sizeof(int) * chunks, stream));
+  for (int ch = 0; ch < chunks; ++ch) {
+    const int kc = (int)std::min<int64_t>(kKC, k - (int64_t)ch * kKC);
+    int* f = flags + (size_t)ch * 2 * (nblk + 1);
+    float* xc = x + ch * kKC;
+    trsv_chain_kernel<float, true, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, ldx, kc, f,
+                                                                              f + nblk, status);
+    RM_LAUNCHED();
+    trsv_chain_kernel<float, false, false><<<nblk, kTrsvThreads, 0, stream>>>(lu, ld, (int)n, dinv, xc, ldx, kc,
+                                                                               f + nblk + 1, f + 2 * nblk + 1, status);
+    RM_LAUNCHED();
+  }
   return RM_OK;
 }
 

@@ -17,12 +17,13 @@ int dgemm_device(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha
 int scale_device(double* c, int64_t ldc, int64_t m, int64_t n, double beta, cudaStream_t stream);
 
 // ---------------------------------------------------------------- FP32 tensor-core GEMM (sgemm_tc.cu)
-// C = alpha A B^T + beta C, A m x k and B n x k K-major (lda, ldb % 4 == 0, 16-byte bases),
-// C row-major. passes 1: TF32 inputs; passes 3: alo/blo hold x - trunc_tf32(x) and three
-// products give float32-level accuracy.
-int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* alo,
-             int64_t ldalo, const float* b, int64_t ldb, const float* blo, int64_t ldblo, float beta, float* c,
-             int64_t ldc, unsigned* status, cudaStream_t stream);
+// C = alpha A B^T + beta C in float32 on tcgen05: A m x k and B n x k row-major (k
+// contiguous), lda, ldb % 4 == 0, 16-byte bases; C row-major, and when ct is not NULL its
+// transpose goes to ct (ldct) too. passes 1: TF32 inputs; passes 3: float32-level products.
+int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* b,
+             int64_t ldb, float beta, float* c, int64_t ldc, unsigned* status, cudaStream_t stream,
+             float* ct = nullptr, int64_t ldct = 0);
+int transpose_f32(const float* src, int64_t lds, int64_t m, int64_t n, float* dst, int64_t ldd, cudaStream_t stream);
 int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStream_t stream);
 int split_lo_f32(const float* x, int64_t ldx, int64_t m, int64_t k, float* lo, int64_t ldl, cudaStream_t stream);
 
@@ -96,6 +97,28 @@ unsigned* device_status();
 // Reads and clears the current device's status word (synchronises `stream`); maps bits to
 // an rm status code.
 int take_device_status(cudaStream_t stream);
+
+// ---------------------------------------------------------------- mixed precision (mixed.cu)
+size_t getrf_genp_f32_scratch_bytes(int64_t n);
+// Unpivoted LU of the row-major float32 n x n a (lda % 4 == 0) with 3xTF32 block updates.
+int getrf_genp_f32(float* a, int64_t lda, int64_t n, void* scratch, unsigned* status, cudaStream_t stream);
+// Random depth-2 butterfly parameters (2N doubles) for size N (a multiple of 4).
+int butterfly_params(double* r, int64_t N, uint64_t seed, cudaStream_t stream);
+// ar (N x N float32) = U^T [A 0; 0 I] V.
+int rbt_matrix(const double* a, int64_t lda, int64_t n, int64_t N, const double* ru, const double* rv, float* ar,
+               int64_t ldr, cudaStream_t stream);
+// c (N x k float32) = U^T [r; 0].
+int rbt_left(const double* r, int64_t ldr, int64_t n, int64_t N, int64_t k, const double* ru, float* c, int64_t ldc,
+             cudaStream_t stream);
+// x (n x k) = (assign) or += rows 0..n-1 of V y.
+int rbt_right_add(const float* y, int64_t ldy, int64_t n, int64_t N, int64_t k, const double* rv, double* x,
+                  int64_t ldx, bool assign, cudaStream_t stream);
+// float32 triangular solves of an unpivoted row-major L\U (getrs.cu)
+size_t diag_blocks_f32_bytes(int64_t n);
+int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream);
+size_t trsv_f32_scratch_bytes(int64_t n, int64_t k);
+int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, float* x, int64_t ldx, int64_t k,
+                       void* scratch, unsigned* status, cudaStream_t stream);
 
 // ---------------------------------------------------------------- helpers (api.cu)
 int64_t round_up(int64_t x, int64_t m);

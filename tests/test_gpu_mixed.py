@@ -1,0 +1,77 @@
+"""The mixed-precision solve (RM_METHOD_F32_IR): butterflies + unpivoted float32 LU on the
+tensor cores + float64 refinement. Its results must meet the plain path's bar: normwise
+backward error <= n * 2^-53, measured here by the oracle's double-double residual, and a
+solution that agrees with the oracle's within the forward error kappa * n * eps allows."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+EPS = np.finfo(np.float64).eps
+
+
+def conditioned(n, k, kappa, seed):
+    """A = U diag(logspace(0, -log10 kappa)) V^T with Haar-like U, V; B ~ N(0,1)."""
+    rng = np.random.default_rng(seed)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    s = np.logspace(0, -np.log10(kappa), n)
+    return (u * s) @ v.T, rng.standard_normal((n, k))
+
+
+@pytest.fixture(scope="module")
+def rb():
+    import rustymath_b200 as rb
+    return rb
+
+
+@pytest.mark.parametrize("n,k,kappa", [(1024, 16, 1e4), (1001, 3, 1e4), (130, 1, 1e3), (17, 2, 10.0), (5, 1, 2.0),
+                                       (2048, 5, 1e4)])
+def test_mixed_meets_the_fp64_bar(rb, n, k, kappa):
+    a, b = conditioned(n, k, kappa, n + k)
+    x, reps = rb.solve_report(a, b, method="mixed")
+    rep = reps[0]
+    assert rep.method_used == 1 and rep.fell_back == 0, "refinement converged without falling back"
+    assert rep.iterations <= 5
+    assert O.backward_error(a, x, b) <= n * 2.0 ** -53
+    xo = O.solve(a, b)
+    assert np.abs(x - xo).max() / np.abs(xo).max() <= kappa * n * EPS
+
+
+def test_mixed_device_tensors(rb):
+    import torch
+    n, k = 600, 4
+    a, b = conditioned(n, k, 1e3, 3)
+    x = rb.solve(torch.tensor(a, device="cuda"), torch.tensor(b, device="cuda"), method="mixed")
+    assert O.backward_error(a, x.cpu().numpy(), b) <= n * 2.0 ** -53
+
+
+def test_mixed_falls_back_when_refinement_stalls(rb):
+    """kappa = 1e12 is beyond float32 factors' reach (kappa * u >> 1): refinement stalls and
+    the plain float64 LU answers, as the report says."""
+    n, k = 300, 2
+    a, b = conditioned(n, k, 1e12, 5)
+    x, reps = rb.solve_report(a, b, method="mixed")
+    assert reps[0].fell_back == 1 and reps[0].method_used == 0
+    assert O.backward_error(a, x, b) <= n * 2.0 ** -53
+
+
+def test_mixed_singular_matrix_is_not_regular(rb):
+    """A singular matrix: refinement fails, the fallback applies rustymath's regular test."""
+    a = np.ones((8, 8))
+    with pytest.raises(rb.NotRegular):
+        rb.solve(a, np.ones(8), method="mixed")
+
+
+def test_mixed_without_fallback_reports_no_convergence(rb):
+    import ctypes
+    from rustymath_b200 import _lib
+    n, k = 200, 1
+    a, b = conditioned(n, k, 1e12, 7)
+    x = np.zeros((n, k))
+    opts = rb.linalg._options("mixed", fallback=False)
+    rep = _lib.SolveReport()
+    st = _lib.load().rm_dsolve_host(n, a.ctypes.data, b.ctypes.data, k, x.ctypes.data, ctypes.byref(opts),
+                                    ctypes.byref(rep))
+    assert st == _lib.RM_NO_CONVERGENCE
