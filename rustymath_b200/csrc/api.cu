@@ -568,12 +568,12 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   return take_device_status(s);
 }
 
-// The mixed-precision solve: butterflies, unpivoted float32 LU on the tensor cores, float64
-// refinement until the backward error reaches the tolerance; stalls fall back to the plain
-// float64 solve (when opts->fallback) or return RM_NO_CONVERGENCE.
+// The mixed-precision solve: float32 LU on the tensor cores (panels pivoted among their own
+// 256 rows), then float64 refinement until the backward error reaches the tolerance; a stall
+// falls back to the plain float64 solve (opts->fallback) or returns RM_NO_CONVERGENCE.
 static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t k, double* d_x,
                         const rm_solve_options* opts, rm_solve_report* report, cudaStream_t s) {
-  const int64_t N = round_up(n, 4), ldr = round_up(N, 32);
+  const int64_t ldf = round_up(n, 32);
   const double tol = opts->tolerance > 0.0 ? opts->tolerance : (double)n * 0x1.0p-53;
   const int max_it = opts->max_iterations > 0 ? opts->max_iterations : 30;
   int iterations = 0;
@@ -581,44 +581,42 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
   double berr_h = 0.0;
   {
     Arena ar;
-    const size_t oar = ar.add((size_t)N * ldr * 4), oru = ar.add((size_t)2 * N * 8), orv = ar.add((size_t)2 * N * 8);
-    const size_t olu = ar.add(getrf_genp_f32_scratch_bytes(N)), odinv = ar.add(diag_blocks_f32_bytes(N));
-    const size_t oc = ar.add((size_t)N * k * 4), orr = ar.add((size_t)n * k * 8), onorm = ar.add(residual_norms_bytes(k));
-    const size_t oberr = ar.add(2 * sizeof(double)), otr = ar.add(trsv_f32_scratch_bytes(N, k));
+    const size_t of = ar.add((size_t)n * ldf * 4), operm = ar.add((size_t)n * 4);
+    const size_t olu = ar.add(getrf_lpp_f32_scratch_bytes(n)), odinv = ar.add(diag_blocks_f32_bytes(n));
+    const size_t oc = ar.add((size_t)n * k * 4), orr = ar.add((size_t)n * k * 8), onorm = ar.add(residual_norms_bytes(k));
+    const size_t oberr = ar.add(2 * sizeof(double)), otr = ar.add(trsv_f32_scratch_bytes(n, k));
     Scratch sc;
     sc.stream = s;
     RM_TRY(scratch_alloc(&sc.base, ar.total, s));
-    float* arf = sc.at<float>(oar);
-    const double* ru = sc.at<double>(oru);
-    const double* rv = sc.at<double>(orv);
+    float* f = sc.at<float>(of);
+    int* perm = sc.at<int>(operm);
     float* c = sc.at<float>(oc);
     unsigned* st = device_status();
-    RM_TRY(butterfly_params(sc.at<double>(oru), N, 0x5eed0001ull, s));
-    RM_TRY(butterfly_params(sc.at<double>(orv), N, 0x5eed0002ull, s));
-    RM_TRY(rbt_matrix(d_a, n, n, N, ru, rv, arf, ldr, s));
-    RM_TRY(getrf_genp_f32(arf, ldr, N, sc.at<void>(olu), st, s));
-    RM_TRY(invert_diag_blocks_f32(arf, ldr, N, sc.at<float>(odinv), s));
-    // x0 = V (LU)^-1 U^T b
-    RM_TRY(rbt_left(d_b, k, n, N, k, ru, c, k, s));
-    RM_TRY(lu_solve_f32_nopiv(arf, ldr, N, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
-    RM_TRY(rbt_right_add(c, k, n, N, k, rv, d_x, k, true, s));
+    RM_TRY(to_f32(d_a, n, n, f, ldf, s));
+    RM_TRY(getrf_lpp_f32(f, ldf, n, perm, sc.at<void>(olu), st, s));
+    RM_TRY(invert_diag_blocks_f32(f, ldf, n, sc.at<float>(odinv), s));
+    // x0 = (LU)^-1 P b
+    RM_TRY(gather_f32(d_b, k, perm, n, k, c, k, s));
+    RM_TRY(lu_solve_f32_nopiv(f, ldf, n, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
+    RM_TRY(accumulate_f64(c, k, n, k, d_x, k, true, s));
     double prev = INFINITY;
     for (int it = 0; it <= max_it; ++it) {
       RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
       RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(oberr), s));
       RM_CUDA_TRY(cudaMemcpyAsync(&berr_h, sc.at<double>(oberr), sizeof berr_h, cudaMemcpyDeviceToHost, s));
       const int dst = take_device_status(s);  // synchronises
-      if (dst != RM_OK) return dst;
+      if (dst != RM_OK && dst != RM_TIMEOUT) return dst;
+      if (dst == RM_TIMEOUT) break;
       if (berr_h <= tol) {
         converged = true;
         break;
       }
       if (!(berr_h < 0.5 * prev) || it == max_it) break;  // stalled, diverging, NaN, or out of steps
       prev = berr_h;
-      // x += V (LU)^-1 U^T r
-      RM_TRY(rbt_left(sc.at<double>(orr), k, n, N, k, ru, c, k, s));
-      RM_TRY(lu_solve_f32_nopiv(arf, ldr, N, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
-      RM_TRY(rbt_right_add(c, k, n, N, k, rv, d_x, k, false, s));
+      // x += (LU)^-1 P r
+      RM_TRY(gather_f32(sc.at<double>(orr), k, perm, n, k, c, k, s));
+      RM_TRY(lu_solve_f32_nopiv(f, ldf, n, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
+      RM_TRY(accumulate_f64(c, k, n, k, d_x, k, false, s));
       ++iterations;
     }
   }

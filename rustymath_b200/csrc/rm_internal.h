@@ -99,20 +99,16 @@ unsigned* device_status();
 int take_device_status(cudaStream_t stream);
 
 // ---------------------------------------------------------------- mixed precision (mixed.cu)
-size_t getrf_genp_f32_scratch_bytes(int64_t n);
-// Unpivoted LU of the row-major float32 n x n a (lda % 4 == 0) with 3xTF32 block updates.
-int getrf_genp_f32(float* a, int64_t lda, int64_t n, void* scratch, unsigned* status, cudaStream_t stream);
-// Random depth-2 butterfly parameters (2N doubles) for size N (a multiple of 4).
-int butterfly_params(double* r, int64_t N, uint64_t seed, cudaStream_t stream);
-// ar (N x N float32) = U^T [A 0; 0 I] V.
-int rbt_matrix(const double* a, int64_t lda, int64_t n, int64_t N, const double* ru, const double* rv, float* ar,
-               int64_t ldr, cudaStream_t stream);
-// c (N x k float32) = U^T [r; 0].
-int rbt_left(const double* r, int64_t ldr, int64_t n, int64_t N, int64_t k, const double* ru, float* c, int64_t ldc,
-             cudaStream_t stream);
-// x (n x k) = (assign) or += rows 0..n-1 of V y.
-int rbt_right_add(const float* y, int64_t ldy, int64_t n, int64_t N, int64_t k, const double* rv, double* x,
-                  int64_t ldx, bool assign, cudaStream_t stream);
+size_t getrf_lpp_f32_scratch_bytes(int64_t n);
+// float32 LU of the row-major n x n a (lda % 4 == 0) with each 128-column panel pivoted among
+// its own 256 rows; perm[i] (int32) = the row of the input that row i of L U comes from.
+int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, unsigned* status, cudaStream_t stream);
+int to_f32(const double* a, int64_t lda, int64_t n, float* f, int64_t ldf, cudaStream_t stream);
+// c (float32) = r[perm]; x (float64) = c or x += c.
+int gather_f32(const double* r, int64_t ldr, const int* perm, int64_t n, int64_t k, float* c, int64_t ldc,
+               cudaStream_t stream);
+int accumulate_f64(const float* c, int64_t ldc, int64_t n, int64_t k, double* x, int64_t ldx, bool assign,
+                   cudaStream_t stream);
 // float32 triangular solves of an unpivoted row-major L\U (getrs.cu)
 size_t diag_blocks_f32_bytes(int64_t n);
 int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream);

@@ -1,5 +1,5 @@
-"""The mixed-precision solve (RM_METHOD_F32_IR): butterflies + unpivoted float32 LU on the
-tensor cores + float64 refinement. Its results must meet the plain path's bar: normwise
+"""The mixed-precision solve (RM_METHOD_F32_IR): float32 LU on the tensor cores with panels
+pivoted among their own 256 rows, then float64 refinement. Its results must meet the plain path's bar: normwise
 backward error <= n * 2^-53, measured here by the oracle's double-double residual, and a
 solution that agrees with the oracle's within the forward error kappa * n * eps allows."""
 import numpy as np
