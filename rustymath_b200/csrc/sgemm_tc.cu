@@ -9,11 +9,18 @@
 // TMEM; the dropped A_lo B_lo term is ~2^-22 relative. The low parts are formed in shared
 // memory from the tiles TMA brought in, so the operands cross L2 once.
 //
-// Warp roles (192 threads): warp 0 issues the TMA loads (128-byte swizzle, 3-stage ring),
-// warp 1 owns the TMEM allocation and its lane 0 issues the MMAs (M=128, N=128, K=8 per
-// instruction) and commits each stage back to the producer, warps 2..5 form the low parts
-// of each stage (three passes), then read the 128 x 128 accumulator out of TMEM (one
-// 32-lane quarter each) and write C. Every wait is bounded; TMEM is freed on every path.
+// Persistent: a CTA per SM walks the output tiles in a fixed stride. Warp 0 issues the TMA
+// loads (128-byte swizzle) into a ring of stages; warp 1 owns the TMEM allocation (two
+// 128 x 128 FP32 accumulators) and its lane 0 issues the MMAs (M=128, N=128, K=8 per
+// instruction), alternating accumulators between tiles so that the next tile's MMAs run
+// while the epilogue drains the last one; warps 2..5 are the epilogue (one 32-lane TMEM
+// quarter each), in 32 x 32 chunks: C's chunk comes in by TMA one chunk ahead (when beta is
+// not zero), alpha*acc + beta*C is formed in the same swizzled shared-memory buffer and goes
+// out as an asynchronous TMA store, so no global access stalls these warps; the optional
+// transposed copy is written from registers in coalesced columns. (When C's address or row
+// stride does not suit TMA, the epilogue stages through shared memory and writes coalesced
+// rows itself.) For three passes warps 6..9 form the low parts of each stage. Every wait is
+// bounded; TMEM is freed on every path.
 #include "rm_internal.h"
 
 namespace rm {
@@ -21,14 +28,22 @@ namespace rm {
 namespace tc {
 
 constexpr int BM = 128, BN = 128, BK = 32;  // BK floats = 128 bytes: one swizzle row
-constexpr int STAGES = 3;
 constexpr int TILE_BYTES = BM * BK * 4;     // 16 KB per operand tile (BM == BN)
-constexpr int THREADS = 192;
-constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t TMEM_COLS = 256;         // two accumulators of BN columns
+constexpr int STG_STRIDE = 33;              // direct epilogue: 32 x 32 floats per warp, padded
+constexpr int EPI_BUF = 32 * 32 * 4;        // TMA epilogue: one 32 x 32 chunk, 128-byte swizzle
+constexpr int STG_BYTES = 4 * 2 * EPI_BUF;  // two chunk buffers per epilogue warp (>= the direct staging)
 
-// UMMA shared-memory descriptor for a K-major tile written by TMA with 128-byte swizzle
-// (box {32 k, 128 rows}): rows of 128 bytes, 8-row groups 1024 bytes apart (stride byte
-// offset), leading byte offset unused (1), descriptor version 1 (sm_100), layout type 2.
+template <int PASSES>
+struct Cfg {
+  static constexpr int OPS = PASSES == 3 ? 4 : 2;  // tiles per stage: A, B, (A_lo, B_lo)
+  static constexpr int STAGES = PASSES == 3 ? 3 : 6;
+  static constexpr int STAGE_BYTES = OPS * TILE_BYTES;
+  static constexpr int LO_WARPS = PASSES == 3 ? 4 : 0;
+  static constexpr int THREADS = 32 * (6 + LO_WARPS);
+  static constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE_BYTES + STG_BYTES + 512;
+};
+
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFF);
@@ -76,38 +91,64 @@ __device__ __forceinline__ uint32_t lo_bits(uint32_t x) {
   return __float_as_uint(v - __uint_as_float(x & 0xFFFFE000u));
 }
 
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(map),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Byte offset of float (row r, column j) in a 32 x 32 chunk written by TMA with 128-byte swizzle.
+__device__ __forceinline__ uint32_t chunk_off(int r, int j) {
+  return (uint32_t)(r * 128 + ((((j >> 2) ^ (r & 7)) << 4) | ((j & 3) << 2)));
+}
+
 }  // namespace tc
 
-template <int PASSES>
-__global__ void __launch_bounds__(tc::THREADS, 1)
+template <int PASSES, bool TMA_EPI>
+__global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
     sgemm_tc_kernel(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
-                    float* __restrict__ c, int64_t ldc, float* __restrict__ ct, int64_t ldct, int m, int n, int k,
-                    float alpha, float beta, unsigned* status) {
+                    const __grid_constant__ CUtensorMap tm_c, float* __restrict__ c, int64_t ldc,
+                    float* __restrict__ ct, int64_t ldct, int m, int n, int k, float alpha, float beta,
+                    unsigned* status) {
   using namespace tc;
-  constexpr int OPS = PASSES == 3 ? 4 : 2;  // tiles per stage: A, B, (A_lo, B_lo)
-  constexpr int STAGE_BYTES = OPS * TILE_BYTES;
+  using C = Cfg<PASSES>;
+  constexpr int S = C::STAGES;
   constexpr int LOAD_BYTES = 2 * TILE_BYTES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* empty = full + STAGES;
-  uint64_t* lo_ready = empty + STAGES;
-  uint64_t* done = lo_ready + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-  __shared__ int failed;
+  float* stg_all = reinterpret_cast<float*>(smem + S * C::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_BYTES + STG_BYTES);
+  uint64_t* empty = full + S;
+  uint64_t* lo_ready = empty + S;
+  uint64_t* tfull = lo_ready + S;   // an accumulator holds a finished tile
+  uint64_t* tempty = tfull + 2;     // the epilogue has read an accumulator out
+  uint64_t* mma_done = tempty + 2;  // every MMA issued has completed
+  uint64_t* cload = mma_done + 1;   // [epilogue warp][buffer]: a chunk of C has landed
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + 8);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int ntn = (n + BN - 1) / BN;
+  const int tiles = ((m + BM - 1) / BM) * ntn;
   const int ktiles = (k + BK - 1) / BK;
 
   if (threadIdx.x == 0) {
-    failed = 0;
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
-      mbar_init(&lo_ready[s], 4);  // one arrival per low-part warp
+      mbar_init(&lo_ready[s], C::LO_WARPS > 0 ? C::LO_WARPS : 1);
     }
-    mbar_init(done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(mma_done, 1);
+    for (int b = 0; b < 8; ++b) mbar_init(&cload[b], 1);
     fence_barrier_init();
   }
   if (warp == 1) {
@@ -121,71 +162,220 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
+    // ---------------- TMA producer
     if (lane == 0) {
       tma_prefetch_desc(&tm_a);
       tma_prefetch_desc(&tm_b);
-      int issued = 0;
-      for (int kt = 0; kt < ktiles; ++kt) {
-        const int s = kt % STAGES;
-        if (!mbar_wait(&empty[s], ((kt / STAGES) & 1u) ^ 1u, status)) {
-          failed = 1;
-          break;
+      int it = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+        for (int kt = 0; kt < ktiles; ++kt, ++it) {
+          const int s = it % S;
+          if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, status)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + s * C::STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], LOAD_BYTES);
+          tma_load_2d(st, &tm_a, &full[s], kt * BK, m0);
+          tma_load_2d(st + TILE_BYTES, &tm_b, &full[s], kt * BK, n0);
         }
-        uint8_t* st = smem + s * STAGE_BYTES;
-        mbar_arrive_expect_tx(&full[s], LOAD_BYTES);
-        const int k0 = kt * BK;
-        tma_load_2d(st, &tm_a, &full[s], k0, m0);
-        tma_load_2d(st + TILE_BYTES, &tm_b, &full[s], k0, n0);
-        ++issued;
       }
       // the copies still in flight land before this thread leaves (bounded)
-      for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
-        mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1u, status);
+      for (int j = (it > S ? it - S : 0); j < it; ++j) mbar_wait(&full[j % S], (j / S) & 1u, status);
     }
   } else if (warp == 1) {
+    // ---------------- MMA issuer
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_tf32(BM, BN);
-      for (int kt = 0; kt < ktiles; ++kt) {
-        const int s = kt % STAGES;
-        const uint32_t par = (kt / STAGES) & 1u;
-        if (!mbar_wait(&full[s], par, status) || (PASSES == 3 && !mbar_wait(&lo_ready[s], par, status))) {
-          failed = 1;
-          break;
-        }
+      int it = 0, lt = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++lt) {
+        const int buf = lt & 1;
+        if (!mbar_wait(&tempty[buf], ((lt >> 1) & 1u) ^ 1u, status)) break;
         tc::fence_after();
-        const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-        const uint32_t sb = sa + TILE_BYTES;
+        const uint32_t d = tmem + buf * BN;
+        for (int kt = 0; kt < ktiles; ++kt, ++it) {
+          const int s = it % S;
+          const uint32_t par = (it / S) & 1u;
+          if (!mbar_wait(&full[s], par, status) || (PASSES == 3 && !mbar_wait(&lo_ready[s], par, status))) {
+            ok = false;
+            break;
+          }
+          tc::fence_after();
+          const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
+          const uint32_t sb = sa + TILE_BYTES;
 #pragma unroll
-        for (int kk = 0; kk < BK / 8; ++kk) {
-          const uint32_t off = kk * 32;  // 8 tf32 = 32 bytes along the swizzled rows
-          const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
-          const uint64_t da = tc::smem_desc(sa + off), db = tc::smem_desc(sb + off);
-          if (PASSES == 3) {
-            const uint64_t dalo = tc::smem_desc(sa + 2 * TILE_BYTES + off);
-            const uint64_t dblo = tc::smem_desc(sa + 3 * TILE_BYTES + off);
-            tc::mma_tf32(tmem, dalo, db, idesc, first);
-            tc::mma_tf32(tmem, da, dblo, idesc, 1u);
-            tc::mma_tf32(tmem, da, db, idesc, 1u);
-          } else {
-            tc::mma_tf32(tmem, da, db, idesc, first);
+          for (int kk = 0; kk < BK / 8; ++kk) {
+            const uint32_t off = kk * 32;  // 8 tf32 = 32 bytes along the swizzled rows
+            const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
+            const uint64_t da = tc::smem_desc(sa + off), db = tc::smem_desc(sb + off);
+            if (PASSES == 3) {
+              const uint64_t dalo = tc::smem_desc(sa + 2 * TILE_BYTES + off);
+              const uint64_t dblo = tc::smem_desc(sa + 3 * TILE_BYTES + off);
+              tc::mma_tf32(d, dalo, db, idesc, first);
+              tc::mma_tf32(d, da, dblo, idesc, 1u);
+              tc::mma_tf32(d, da, db, idesc, 1u);
+            } else {
+              tc::mma_tf32(d, da, db, idesc, first);
+            }
+          }
+          tc::mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
+        }
+        if (ok) tc::mma_commit(&tfull[buf]);  // the accumulator is complete once every MMA above has run
+      }
+      tc::mma_commit(mma_done);
+      mbar_wait(mma_done, 0u, status);
+    }
+  } else if (warp < 6 && TMA_EPI) {
+    // ---------------- epilogue through TMA: warps 2..5, TMEM lane quarter warp % 4
+    const int q = warp & 3, ew = warp - 2;
+    uint8_t* ebuf = reinterpret_cast<uint8_t*>(stg_all) + ew * 2 * EPI_BUF;
+    uint64_t* cl = cload + 2 * ew;
+    const bool load_c = beta != 0.0f;
+    // chunk ci (counted over this CTA's tiles) uses buffer ci & 1
+    auto prefetch = [&](int ci, int tile, int cb) {
+      if (!load_c || tile >= tiles) return;
+      if (lane == 0) {
+        tc::bulk_wait_read<0>();  // the store that last used this buffer has read it
+        const int b = ci & 1;
+        mbar_arrive_expect_tx(&cl[b], EPI_BUF);
+        tma_load_2d(ebuf + b * EPI_BUF, &tm_c, &cl[b], (tile % ntn) * BN + cb, (tile / ntn) * BM + q * 32);
+      }
+      __syncwarp();
+    };
+    int lt = 0, ci = 0;
+    bool ok = true;
+    prefetch(0, blockIdx.x, 0);
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++lt) {
+      const int buf = lt & 1;
+      if (!mbar_wait(&tfull[buf], (lt >> 1) & 1u, status)) break;
+      tc::fence_after();
+      const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+      const int row0 = m0 + q * 32;
+#pragma unroll 1
+      for (int cb = 0; cb < BN; cb += 32, ++ci) {
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * BN + cb, v);
+        if (cb == BN - 32) {  // the accumulator is in registers: hand it back to the MMA warp
+          tc::fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[buf]);
+        }
+        const int b = ci & 1;
+        uint8_t* eb = ebuf + b * EPI_BUF;
+        if (load_c) {
+          if (!mbar_wait(&cl[b], (ci >> 1) & 1u, status)) {
+            ok = false;
+            break;
+          }
+        } else {
+          if (lane == 0) tc::bulk_wait_read<1>();  // the store two chunks back has read this buffer
+          __syncwarp();
+        }
+        // this lane's row of the chunk: alpha * acc + beta * C, in place
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+          float4* p = reinterpret_cast<float4*>(eb + tc::chunk_off(lane, 4 * g));
+          float4 o = make_float4(alpha * __uint_as_float(v[4 * g]), alpha * __uint_as_float(v[4 * g + 1]),
+                                 alpha * __uint_as_float(v[4 * g + 2]), alpha * __uint_as_float(v[4 * g + 3]));
+          if (load_c) {
+            const float4 cv = *p;
+            o.x = fmaf(beta, cv.x, o.x), o.y = fmaf(beta, cv.y, o.y), o.z = fmaf(beta, cv.z, o.z),
+            o.w = fmaf(beta, cv.w, o.w);
+          }
+          *p = o;
+          if (ct) {
+            // the transposed copy: column j of the chunk, the warp's 32 rows in 32 consecutive floats
+            const int row = row0 + lane;
+            const float ov[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int col = n0 + cb + 4 * g + e;
+              if (row < m && col < n) ct[(int64_t)col * ldct + row] = ov[e];
+            }
           }
         }
-        tc::mma_commit(&empty[s]);  // the stage is free once these MMAs have read it
+        fence_proxy_async();  // the TMA store reads these through the async proxy
+        __syncwarp();
+        if (lane == 0) {
+          tc::tma_store_2d(&tm_c, eb, n0 + cb, row0);
+          tc::bulk_commit();
+        }
+        // the next chunk of C (this tile's, or the next tile's first)
+        if (cb + 32 < BN) prefetch(ci + 1, tile, cb + 32);
+        else prefetch(ci + 1, tile + gridDim.x, 0);
       }
-      tc::mma_commit(done);  // the accumulator is complete once every MMA above has run
     }
-  } else {
-    // ---------------- warps 2..5: the low parts of each stage, then the epilogue
-    const int t = threadIdx.x - 64;  // 0..127
-    if (PASSES == 3) {
-      for (int kt = 0; kt < ktiles; ++kt) {
-        const int s = kt % STAGES;
-        if (!mbar_wait(&full[s], (kt / STAGES) & 1u, status)) {
-          failed = 1;
+    if (lane == 0) tc::bulk_wait_all();  // every store has landed before the CTA ends
+    __syncwarp();
+  } else if (warp < 6) {
+    // ---------------- epilogue, direct: warps 2..5, TMEM lane quarter warp % 4
+    const int q = warp & 3;
+    float* stg = stg_all + (warp - 2) * 32 * STG_STRIDE;
+    int lt = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++lt) {
+      const int buf = lt & 1;
+      if (!mbar_wait(&tfull[buf], (lt >> 1) & 1u, status)) break;
+      tc::fence_after();
+      const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+      const int row0 = m0 + q * 32;
+#pragma unroll 1
+      for (int cb = 0; cb < BN; cb += 32) {
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * BN + cb, v);
+        if (cb == BN - 32) {  // the accumulator is in registers: hand it back to the MMA warp
+          tc::fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[buf]);
+        }
+        __syncwarp();  // the last chunk's reads of the staging tile are done
+#pragma unroll
+        for (int j = 0; j < 32; ++j) stg[lane * STG_STRIDE + j] = __uint_as_float(v[j]);
+        __syncwarp();
+        // lane = column: each row of the chunk is one coalesced 128-byte access
+        const int col = n0 + cb + lane;
+        float cv[32];
+        if (beta != 0.0f) {
+#pragma unroll
+          for (int rr = 0; rr < 32; ++rr) {
+            const int row = row0 + rr;
+            cv[rr] = (row < m && col < n) ? c[(int64_t)row * ldc + col] : 0.0f;
+          }
+        }
+#pragma unroll
+        for (int rr = 0; rr < 32; ++rr) {
+          const int row = row0 + rr;
+          float out = alpha * stg[rr * STG_STRIDE + lane];
+          if (beta != 0.0f) out = fmaf(beta, cv[rr], out);
+          if (row < m && col < n) c[(int64_t)row * ldc + col] = out;
+          if (ct) stg[rr * STG_STRIDE + lane] = out;
+        }
+        if (ct) {
+          // lane = row: each column of the chunk is one coalesced access of the transposed copy
+          __syncwarp();
+          const int row = row0 + lane;
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (row < m && n0 + cb + j < n) ct[(int64_t)(n0 + cb + j) * ldct + row] = stg[lane * STG_STRIDE + j];
+        }
+      }
+    }
+  } else if (PASSES == 3) {
+    // ---------------- warps 6..9: the low parts of each stage
+    const int t = threadIdx.x - 192;  // 0..127
+    int it = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+      for (int kt = 0; kt < ktiles; ++kt, ++it) {
+        const int s = it % S;
+        if (!mbar_wait(&full[s], (it / S) & 1u, status)) {
+          ok = false;
           break;
         }
-        const uint4* src = reinterpret_cast<const uint4*>(smem + s * STAGE_BYTES);
-        uint4* dst = reinterpret_cast<uint4*>(smem + s * STAGE_BYTES + 2 * TILE_BYTES);
+        const uint4* src = reinterpret_cast<const uint4*>(smem + s * C::STAGE_BYTES);
+        uint4* dst = reinterpret_cast<uint4*>(smem + s * C::STAGE_BYTES + 2 * TILE_BYTES);
 #pragma unroll 4
         for (int i = t; i < 2 * TILE_BYTES / 16; i += 128) {  // A then B: same swizzled positions
           const uint4 v = src[i];
@@ -196,32 +386,8 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
         if (lane == 0) mbar_arrive(&lo_ready[s]);
       }
     }
-    const int q = warp & 3;
-    const bool ready = mbar_wait(done, 0u, status);
-    tc::fence_after();
-    const int row = m0 + q * 32 + lane;
-    if (ready && !failed && ktiles > 0) {
-#pragma unroll 1
-      for (int cb = 0; cb < BN; cb += 32) {
-        uint32_t v[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + cb, v);
-        if (row < m) {
-          float* crow = c + (int64_t)row * ldc + n0 + cb;
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            if (n0 + cb + j < n) {
-              const float d = __uint_as_float(v[j]);
-              const float out = beta == 0.0f ? alpha * d : fmaf(beta, crow[j], alpha * d);
-              crow[j] = out;
-              // the transposed copy: the warp's 32 rows land in 32 consecutive floats
-              if (ct) ct[(int64_t)(n0 + cb + j) * ldct + row] = out;
-            }
-          }
-        }
-      }
-    }
-    tc::fence_before();
   }
+  tc::fence_before();
   __syncthreads();
   if (warp == 1) {
     tc::fence_after();
@@ -265,22 +431,21 @@ int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStrea
   return RM_OK;
 }
 
-size_t sgemm_tc_smem(int passes) {
-  return (size_t)tc::STAGES * (passes == 3 ? 4 : 2) * tc::TILE_BYTES + 1024 + 512;
-}
-
-template <int PASSES>
-static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, float* c, int64_t ldc, float* ct, int64_t ldct,
-                        int m, int n, int k, float alpha, float beta, unsigned* status, cudaStream_t stream) {
-  const size_t smem = sgemm_tc_smem(PASSES);
+template <int PASSES, bool TMA_EPI>
+static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tcm, float* c, int64_t ldc,
+                        float* ct, int64_t ldct, int m, int n, int k, float alpha, float beta, unsigned* status,
+                        cudaStream_t stream) {
+  using C = tc::Cfg<PASSES>;
   static bool set = false;
   if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tc_kernel<PASSES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tc_kernel<PASSES, TMA_EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)C::SMEM));
     set = true;
   }
-  dim3 grid((unsigned)((n + tc::BN - 1) / tc::BN), (unsigned)((m + tc::BM - 1) / tc::BM));
-  sgemm_tc_kernel<PASSES><<<grid, tc::THREADS, smem, stream>>>(ta, tb, c, ldc, ct, ldct, m, n, k, alpha, beta,
-                                                               status);
+  const int64_t tiles = (int64_t)((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN);
+  const unsigned grid = (unsigned)std::min<int64_t>(tiles, device_sm_count());
+  sgemm_tc_kernel<PASSES, TMA_EPI><<<grid, C::THREADS, C::SMEM, stream>>>(ta, tb, tcm, c, ldc, ct, ldct, m, n, k,
+                                                                          alpha, beta, status);
   RM_LAUNCHED();
   return RM_OK;
 }
@@ -294,9 +459,18 @@ int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const flo
   CUtensorMap ta, tb;
   RM_TRY(make_tensor_map_2d(&ta, a, 4, k, m, lda * 4, tc::BK, tc::BM, true));
   RM_TRY(make_tensor_map_2d(&tb, b, 4, k, n, ldb * 4, tc::BK, tc::BN, true));
+  // C through TMA when its base and row stride are 16-byte aligned (the transposed copy,
+  // written directly, only beside beta == 0)
+  CUtensorMap tcm;
+  const bool tma_epi = (reinterpret_cast<uintptr_t>(c) & 15) == 0 && (ldc * 4) % 16 == 0 && !(ct && beta != 0.0f);
+  if (tma_epi) RM_TRY(make_tensor_map_2d(&tcm, c, 4, n, m, ldc * 4, 32, 32, true));
+  else memset(&tcm, 0, sizeof tcm);
   const int mi = (int)m, ni = (int)n, ki = (int)k;
-  if (passes == 3) return launch_sgemm<3>(ta, tb, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream);
-  return launch_sgemm<1>(ta, tb, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream);
+  if (passes == 3)
+    return tma_epi ? launch_sgemm<3, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream)
+                   : launch_sgemm<3, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream);
+  return tma_epi ? launch_sgemm<1, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream)
+                 : launch_sgemm<1, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream);
 }
 
 // dst (n x m, ldd) = src^T for the m x n row-major float32 src (lds): 32x32 tiles through

@@ -31,7 +31,8 @@ def run(passes, a, b, c, alpha, beta, transb=True):
 
 @pytest.mark.parametrize("transb", [True, False])
 @pytest.mark.parametrize("m,n,k", [(128, 128, 32), (64, 64, 8), (129, 130, 33), (300, 257, 100), (1000, 520, 128),
-                                   (256, 384, 1024), (1, 1, 1), (7, 200, 5)])
+                                   (256, 384, 1024), (1, 1, 1), (7, 200, 5),
+                                   (2304, 2200, 96)])  # more tiles than SMs: both accumulators cycle
 def test_sgemm_tc_accuracy(m, n, k, transb):
     rng = np.random.default_rng(m + n + k)
     a = rng.uniform(-1, 1, (m, k)).astype(np.float32)
