@@ -2,6 +2,8 @@
 // plain float64 path. Every entry point returns an rm status code; nothing here falls back
 // to the CPU.
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -528,6 +530,44 @@ int rm_dlu_solve_host(int64_t n, const double* h_factors, const int64_t* h_perm,
 }
 
 // The plain float64 solve: LU, LuWork::regular's test, then the two triangular solves.
+// Phase timing for the solves, on when the environment sets RM_TRACE: CUDA events recorded
+// on the solve's stream between phases, printed to stderr once the solve has synchronised.
+struct PhaseTrace {
+  static constexpr int kMax = 96;
+  bool on = false;
+  int count = 0;
+  cudaEvent_t ev[kMax];
+  const char* name[kMax];
+  cudaStream_t stream;
+  PhaseTrace(cudaStream_t s, const char* what) : stream(s) {
+    static const bool enabled = std::getenv("RM_TRACE") != nullptr;
+    on = enabled;
+    if (on) {
+      std::fprintf(stderr, "rm trace: %s\n", what);
+      mark("start");
+    }
+  }
+  void mark(const char* what) {
+    if (!on || count == kMax) return;
+    if (cudaEventCreate(&ev[count]) != cudaSuccess) return;
+    name[count] = what;
+    cudaEventRecord(ev[count++], stream);
+  }
+  ~PhaseTrace() {
+    if (!on) return;
+    cudaEventSynchronize(ev[count - 1]);
+    float total = 0.0f;
+    for (int i = 1; i < count; ++i) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev[i - 1], ev[i]);
+      total += ms;
+      std::fprintf(stderr, "  %-14s %9.3f ms\n", name[i], ms);
+    }
+    std::fprintf(stderr, "  %-14s %9.3f ms\n", "total", total);
+    for (int i = 0; i < count; ++i) cudaEventDestroy(ev[i]);
+  }
+};
+
 static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t k, double* d_x,
                         rm_solve_report* report, cudaStream_t s) {
   Arena ar;
@@ -539,9 +579,12 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   sc.stream = s;
   RM_TRY(scratch_alloc(&sc.base, ar.total, s));
   double* w = sc.at<double>(lb.w);
+  PhaseTrace tr(s, "plain float64 solve");
   RM_TRY(load_matrix_f64(d_a, n, w, lb.ldw, n, sc.at<double>(lb.amax), s));
+  tr.mark("load");
   RM_TRY(getrf_f64(w, lb.ldw, n, sc.at<int64_t>(lb.ipiv), sc.at<int64_t>(lb.perm), sc.at<void>(lb.getrf),
                    device_status(), s));
+  tr.mark("getrf");
   RM_TRY(regular_flag_f64(w, lb.ldw, n, sc.at<double>(lb.amax), sc.at<int32_t>(lb.flag), s));
   int32_t regular = 0;
   RM_CUDA_TRY(cudaMemcpyAsync(&regular, sc.at<int32_t>(lb.flag), sizeof regular, cudaMemcpyDeviceToHost, s));
@@ -552,12 +595,15 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
     return RM_NOT_REGULAR;
   }
   RM_TRY(invert_diag_blocks_f64(w, lb.ldw, false, n, sc.at<double>(lb.dinv), true, false, s));
+  tr.mark("regular");
   RM_TRY(getrs_f64(w, lb.ldw, false, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k,
                    sc.at<void>(os), device_status(), s));
+  tr.mark("getrs");
   if (report) {
     double berr[2] = {0, 0};
     RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
     RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(lb.berr), s));
+    tr.mark("residual");
     RM_CUDA_TRY(cudaMemcpyAsync(berr, sc.at<double>(lb.berr), sizeof berr, cudaMemcpyDeviceToHost, s));
     RM_TRY(take_device_status(s));
     report->backward_error = berr[0];
@@ -585,6 +631,7 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
     const size_t olu = ar.add(getrf_lpp_f32_scratch_bytes(n)), odinv = ar.add(diag_blocks_f32_bytes(n));
     const size_t oc = ar.add((size_t)n * k * 4), orr = ar.add((size_t)n * k * 8), onorm = ar.add(residual_norms_bytes(k));
     const size_t oberr = ar.add(2 * sizeof(double)), otr = ar.add(trsv_f32_scratch_bytes(n, k));
+    const size_t opre = ar.add(premultiplied_f32_bytes(n));
     Scratch sc;
     sc.stream = s;
     RM_TRY(scratch_alloc(&sc.base, ar.total, s));
@@ -592,17 +639,25 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
     int* perm = sc.at<int>(operm);
     float* c = sc.at<float>(oc);
     unsigned* st = device_status();
+    PhaseTrace tr(s, "mixed float32 + float64 refinement solve");
     RM_TRY(to_f32(d_a, n, n, f, ldf, s));
+    tr.mark("to_f32");
     RM_TRY(getrf_lpp_f32(f, ldf, n, perm, sc.at<void>(olu), st, s));
+    tr.mark("getrf_f32");
     RM_TRY(invert_diag_blocks_f32(f, ldf, n, sc.at<float>(odinv), s));
+    float* pre = n > 1024 ? sc.at<float>(opre) : nullptr;  // worth its one-off cost on long chains
+    if (pre) RM_TRY(premultiply_f32(f, ldf, n, sc.at<float>(odinv), pre, s));
+    tr.mark("solve_setup");
     // x0 = (LU)^-1 P b
     RM_TRY(gather_f32(d_b, k, perm, n, k, c, k, s));
-    RM_TRY(lu_solve_f32_nopiv(f, ldf, n, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
+    RM_TRY(lu_solve_f32_nopiv(f, ldf, n, sc.at<float>(odinv), pre, c, k, k, sc.at<void>(otr), st, s));
     RM_TRY(accumulate_f64(c, k, n, k, d_x, k, true, s));
+    tr.mark("solve");
     double prev = INFINITY;
     for (int it = 0; it <= max_it; ++it) {
       RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
       RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(oberr), s));
+      tr.mark("residual");
       RM_CUDA_TRY(cudaMemcpyAsync(&berr_h, sc.at<double>(oberr), sizeof berr_h, cudaMemcpyDeviceToHost, s));
       const int dst = take_device_status(s);  // synchronises
       if (dst != RM_OK && dst != RM_TIMEOUT) return dst;
@@ -615,8 +670,9 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
       prev = berr_h;
       // x += (LU)^-1 P r
       RM_TRY(gather_f32(sc.at<double>(orr), k, perm, n, k, c, k, s));
-      RM_TRY(lu_solve_f32_nopiv(f, ldf, n, sc.at<float>(odinv), c, k, k, sc.at<void>(otr), st, s));
+      RM_TRY(lu_solve_f32_nopiv(f, ldf, n, sc.at<float>(odinv), pre, c, k, k, sc.at<void>(otr), st, s));
       RM_TRY(accumulate_f64(c, k, n, k, d_x, k, false, s));
+      tr.mark("solve");
       ++iterations;
     }
   }

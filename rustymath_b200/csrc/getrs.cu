@@ -20,7 +20,8 @@ constexpr int kTB32 = 128;          // float32 block rows
 size_t diag_blocks_f64_bytes(int64_t n) { return diag_blocks_bytes_max(n); }
 
 // dinv[b][0] = inverse of the lower diagonal block b, dinv[b][1] = inverse of the upper
-// diagonal block b (row-major TB x TB; rows/columns past n are identity). A unit triangle
+// diagonal block b (row-major TB x TB; rows/columns past n are identity); dinv[b][2..3] are
+// the couplings that coupling_kernel fills in. A unit triangle
 // takes its diagonal as 1 without reading it. The triangles are those of the n x n matrix
 // T whose item (i, j) is w[i*ldw + j], or w[j*ldw + i] when COLMAJOR. Thread c solves for
 // column c of the inverse.
@@ -56,8 +57,83 @@ __global__ void __launch_bounds__(TB) invert_diag_blocks_kernel(const T* __restr
     }
   }
   __syncthreads();
-  T* out = dinv + ((int64_t)b * 2 + which) * TB * TB;
+  T* out = dinv + ((int64_t)b * kDiagMats + which) * TB * TB;
   for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) out[e] = x[e / TB][e % TB];
+}
+
+// out (TB x TB, row-major, ld ldo) = dinv block dv (TB x TB row-major) times block (b, pb) of
+// the n x n matrix T (item (i, j) at w[i*ldw + j], or at w[j*ldw + i] when COLMAJOR; past n,
+// zero). 256 threads, each a (TB/16)^2 piece; smem holds both operands.
+template <typename T, bool COLMAJOR, int TB>
+__device__ __forceinline__ void block_product(const T* __restrict__ w, int64_t ldw, int64_t n, int b, int pb,
+                                              const T* __restrict__ dv, T* __restrict__ out, int64_t ldo) {
+  constexpr int R = TB / 16;
+  extern __shared__ uint8_t smraw[];
+  T(*di)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(smraw);
+  T(*ob)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(smraw + (size_t)TB * (TB + 1) * sizeof(T));
+  const int64_t r0 = (int64_t)b * TB, c0 = (int64_t)pb * TB;
+  for (int e = threadIdx.x; e < TB * TB; e += 256) {
+    const int i = e / TB, j = e % TB;
+    di[i][j] = dv[e];
+    // COLMAJOR storage read down its columns (coalesced)
+    const int ri = COLMAJOR ? j : i, cj = COLMAJOR ? i : j;
+    const int64_t gi = r0 + ri, gj = c0 + cj;
+    ob[ri][cj] = (gi < n && gj < n) ? (COLMAJOR ? w[gj * ldw + gi] : w[gi * ldw + gj]) : T(0);
+  }
+  __syncthreads();
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+  T acc[R][R];
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) acc[i][j] = T(0);
+  for (int q = 0; q < TB; ++q) {
+    T dvv[R], ov[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) dvv[i] = di[ty + 16 * i][q];
+#pragma unroll
+    for (int j = 0; j < R; ++j) ov[j] = ob[q][tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int j = 0; j < R; ++j) acc[i][j] = fma(dvv[i], ov[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) out[(int64_t)(ty + 16 * i) * ldo + tx + 16 * j] = acc[i][j];
+}
+
+// dinv[b][2] = dinv[b][0] T[b, b-1] and dinv[b][3] = dinv[b][1] T[b, b+1]: the coupling of
+// block b to the block the forward (backward) solve finishes just before it, so that block
+// b's last step is x_b = z_b - coupling x_prev with z_b formed while it waits. A CTA per
+// (block, triangle).
+template <typename T, bool COLMAJOR, int TB>
+__global__ void __launch_bounds__(256) coupling_kernel(const T* __restrict__ w, int64_t ldw, int64_t n,
+                                                       T* __restrict__ dinv) {
+  const int b = blockIdx.x, which = blockIdx.y;  // 0: lower (block b-1), 1: upper (block b+1)
+  const int nblk = (int)((n + TB - 1) / TB);
+  const int pb = which == 0 ? b - 1 : b + 1;
+  if (pb < 0 || pb >= nblk) return;
+  block_product<T, COLMAJOR, TB>(w, ldw, n, b, pb, dinv + ((int64_t)b * kDiagMats + which) * TB * TB,
+                                 dinv + ((int64_t)b * kDiagMats + 2 + which) * TB * TB, TB);
+}
+
+// pre = the block-Jacobi-scaled triangles of the row-major L\U w: block (b, j) of pre is
+// dinv[b][0] L_bj below the diagonal blocks (j < b) and dinv[b][1] U_bj above them (j > b);
+// the diagonal blocks of pre are not written. With them a triangular solve is
+// x_b = D_b^-1 y_b - sum_j pre_bj x_j: every block's last step is a single product.
+template <typename T, int TB>
+__global__ void __launch_bounds__(256) premultiply_kernel(const T* __restrict__ w, int64_t ldw, int64_t n,
+                                                          const T* __restrict__ dinv, T* __restrict__ pre,
+                                                          int64_t ldp) {
+  const int nblk = (int)((n + TB - 1) / TB);
+  const int b = blockIdx.x / nblk, j = blockIdx.x % nblk;
+  if (b == j) return;
+  const int which = j < b ? 0 : 1;
+  // rows/columns past n land in the padding of pre (ldp >= nblk * TB, rows allocated likewise)
+  block_product<T, false, TB>(w, ldw, n, b, j, dinv + ((int64_t)b * kDiagMats + which) * TB * TB,
+                              pre + (int64_t)b * TB * ldp + (int64_t)j * TB, ldp);
 }
 
 template <typename T, bool COLMAJOR, int TB>
@@ -68,11 +144,17 @@ static int launch_invert(const T* w, int64_t ldw, int64_t n, T* dinv, bool lower
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(invert_diag_blocks_kernel<T, COLMAJOR, TB>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RM_CUDA_TRY(cudaFuncSetAttribute(coupling_kernel<T, COLMAJOR, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(2 * smem)));
     set = true;
   }
   dim3 grid((unsigned)((n + TB - 1) / TB), 2);
   invert_diag_blocks_kernel<T, COLMAJOR, TB><<<grid, TB, smem, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
   RM_LAUNCHED();
+  if (grid.x > 1) {
+    coupling_kernel<T, COLMAJOR, TB><<<grid, 256, 2 * smem, stream>>>(w, ldw, n, dinv);
+    RM_LAUNCHED();
+  }
   return RM_OK;
 }
 
@@ -94,11 +176,17 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 
 // Solves T x = y for kc <= kKC columns of y (in place in x), T the lower (LOWER) or upper
 // triangle of the matrix whose item (i, j) is w[i*ldw + j] (w[j*ldw + i] when COLMAJOR),
-// in block rows of TB; the diagonal blocks' inverses come from dinv. flags[nblk] and
-// counter start at zero. Thread t owns row t / 4 and columns 4 (t % 4) .. +3 of its block's
-// running sums. The next dependency's block of T is loaded into registers while the current
-// one is applied, so each block of T crosses HBM once, overlapped with the arithmetic.
-template <typename T, bool LOWER, bool COLMAJOR, int TB>
+// in block rows of TB; dinv holds each block's diagonal inverse and its coupling to the
+// block solved just before it. With PRE, w holds the block-Jacobi-scaled triangles
+// (premultiply_kernel): block b forms D_b^-1 y_b first and subtracts pre_bj x_j as each x_j
+// is released. flags[nblk] and counter start at zero. CTAs take tickets in
+// launch order and block rows in solve order; block b subtracts T_bj x_j for every block j
+// solved before it but the last, as each x_j is released, then forms z_b = D_b^-1 (...) and,
+// once the last one (p) is released, x_b = z_b - (D_b^-1 T_bp) x_p: one TB x TB product
+// between seeing p's flag and releasing its own. Thread t owns row t / 4 and columns
+// 4 (t % 4) .. +3 of its block's sums. The next matrix a step needs is loaded into registers
+// while the current one is applied, so each block of T crosses HBM once.
+template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE>
 __global__ void __launch_bounds__(TB * 4)
     trsv_chain_kernel(const T* __restrict__ w, int64_t ldw, int n, const T* __restrict__ dinv, T* x, int64_t ldx,
                       int kc, int* flags, int* counter, unsigned* status) {
@@ -117,6 +205,7 @@ __global__ void __launch_bounds__(TB * 4)
   const int b = LOWER ? t : nblk - 1 - t;
   const int r0 = b * TB, rows = min(TB, n - r0);
   const int my_r = tid >> 2, my_c = (tid & 3) * 4;
+  auto dep = [&](int s) { return LOWER ? s : nblk - 1 - s; };  // the s-th block solved
 
   T acc[4];
 #pragma unroll
@@ -124,23 +213,14 @@ __global__ void __launch_bounds__(TB * 4)
     const int c = my_c + i;
     acc[i] = (my_r < rows && c < kc) ? x[(int64_t)(r0 + my_r) * ldx + c] : T(0);
   }
-  // element e of a block: COLMAJOR storage is read along its columns (coalesced)
-  auto coord = [&](int e, int& r, int& c) {
-    if (COLMAJOR) {
-      c = e / TB;
-      r = e % TB;
-    } else {
-      r = e / TB;
-      c = e % TB;
-    }
-  };
   T regs[LPT];
+  // a block of T: COLMAJOR storage is read along its columns (coalesced)
   auto load = [&](int j) {
     const int c0 = j * TB, cols = min(TB, n - c0);
 #pragma unroll
     for (int q = 0; q < LPT; ++q) {
-      int r, c;
-      coord(tid + q * THREADS, r, c);
+      const int e = tid + q * THREADS;
+      const int r = COLMAJOR ? e % TB : e / TB, c = COLMAJOR ? e / TB : e % TB;
       regs[q] = (r < rows && c < cols)
                     ? (COLMAJOR ? __ldcs(w + (int64_t)(c0 + c) * ldw + r0 + r) : __ldcs(w + (int64_t)(r0 + r) * ldw + c0 + c))
                     : T(0);
@@ -149,9 +229,22 @@ __global__ void __launch_bounds__(TB * 4)
   auto store = [&]() {
 #pragma unroll
     for (int q = 0; q < LPT; ++q) {
-      int r, c;
-      coord(tid + q * THREADS, r, c);
+      const int e = tid + q * THREADS;
+      const int r = COLMAJOR ? e % TB : e / TB, c = COLMAJOR ? e / TB : e % TB;
       lblk[r][c] = regs[q];
+    }
+  };
+  // a row-major matrix of dinv (the diagonal inverse, m = 0, or the coupling, m = 2)
+  auto load_mat = [&](int m) {
+    const T* dv = dinv + ((int64_t)b * kDiagMats + m + (LOWER ? 0 : 1)) * TB * TB;
+#pragma unroll
+    for (int q = 0; q < LPT; ++q) regs[q] = __ldg(dv + tid + q * THREADS);
+  };
+  auto store_mat = [&]() {
+#pragma unroll
+    for (int q = 0; q < LPT; ++q) {
+      const int e = tid + q * THREADS;
+      lblk[e / TB][e % TB] = regs[q];
     }
   };
   // acc[i] += sign * sum_q lblk[my_r][q] xs[q][my_c + i]
@@ -163,22 +256,8 @@ __global__ void __launch_bounds__(TB * 4)
       for (int i = 0; i < 4; ++i) acc[i] = fma(l, xs[q][my_c + i], acc[i]);
     }
   };
-  // the inverse of this block's diagonal block, row-major, prefetched behind the last dependency
-  const T* dv = dinv + ((int64_t)b * 2 + (LOWER ? 0 : 1)) * TB * TB;
-  auto load_dinv = [&]() {
-#pragma unroll
-    for (int q = 0; q < LPT; ++q) regs[q] = __ldg(dv + tid + q * THREADS);
-  };
-  bool ok = true;
-  if (t > 0) load(LOWER ? 0 : nblk - 1);
-  else load_dinv();
-  for (int s = 0; s < t; ++s) {
-    const int j = LOWER ? s : nblk - 1 - s;  // a solved block, in solve order
-    const int c0 = j * TB, cols = min(TB, n - c0);
-    __syncthreads();  // the previous step's reads of lblk / xs are done
-    store();
-    if (s + 1 < t) load(LOWER ? s + 1 : nblk - 2 - s);
-    else load_dinv();
+  // waits (bounded) for block j's release, then stages x_j in xs
+  auto fetch = [&](int j) -> bool {
     if (tid == 0) {
       bool seen = ld_acquire(&flags[j]) != 0;
       if (!seen) {
@@ -191,54 +270,105 @@ __global__ void __launch_bounds__(TB * 4)
       good = seen ? 1 : 0;
     }
     __syncthreads();
-    if (!good) {
-      ok = false;
-      break;
-    }
+    if (!good) return false;
+    const int c0 = j * TB, cols = min(TB, n - c0);
     for (int e = tid; e < TB * kKC; e += THREADS) {
       const int r = e / kKC, c = e % kKC;
       xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : T(0);
     }
     __syncthreads();
-    apply(T(-1));
-  }
-  __syncthreads();
-  if (ok) {
-#pragma unroll
-    for (int q = 0; q < LPT; ++q) {
-      const int e = tid + q * THREADS;
-      lblk[e / TB][e % TB] = regs[q];
-    }
+    return true;
+  };
+
+  bool ok = true;
+  if (PRE) {
+    load_mat(0);
+    store_mat();
+    if (t >= 1) load(dep(0));
 #pragma unroll
     for (int i = 0; i < 4; ++i) xs[my_r][my_c + i] = acc[i];
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i] = T(0);
-    apply(T(1));
+    apply(T(1));  // D_b^-1 y_b
+    for (int s = 0; s < t; ++s) {
+      __syncthreads();
+      store();
+      if (s + 1 < t) load(dep(s + 1));
+      if (!fetch(dep(s))) {
+        ok = false;
+        break;
+      }
+      apply(T(-1));
+    }
+    if (ok) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int c = my_c + i;
-      if (my_r < rows && c < kc) x[(int64_t)(r0 + my_r) * ldx + c] = acc[i];
+      for (int i = 0; i < 4; ++i) {
+        const int c = my_c + i;
+        if (my_r < rows && c < kc) x[(int64_t)(r0 + my_r) * ldx + c] = acc[i];
+      }
+    }
+  } else {
+  if (t >= 2) load(dep(0));
+  else load_mat(0);
+  for (int s = 0; s + 1 < t; ++s) {  // every block solved before this one but the last
+    __syncthreads();                 // the previous step's reads of lblk / xs are done
+    store();
+    if (s + 2 < t) load(dep(s + 1));
+    else load_mat(0);
+    if (!fetch(dep(s))) {
+      ok = false;
+      break;
+    }
+    apply(T(-1));
+  }
+  if (ok) {
+    // z_b = D_b^-1 (y_b - sum ...), while the last block before this one may still be running
+    __syncthreads();
+    store_mat();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) xs[my_r][my_c + i] = acc[i];
+    if (t >= 1) load_mat(2);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[i] = T(0);
+    apply(T(1));
+    if (t >= 1) {
+      __syncthreads();
+      store_mat();
+      if (fetch(dep(t - 1))) apply(T(-1));  // x_b = z_b - C_b x_prev
+      else ok = false;
+    }
+    if (ok) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int c = my_c + i;
+        if (my_r < rows && c < kc) x[(int64_t)(r0 + my_r) * ldx + c] = acc[i];
+      }
     }
   }
-  __threadfence();
+  }
+  // every thread's x is written before the barrier; one fence makes them visible device-wide
   __syncthreads();
-  if (tid == 0) st_release(&flags[b], 1);
+  if (tid == 0) {
+    __threadfence();
+    st_release(&flags[b], 1);
+  }
 }
 
-template <typename T, bool LOWER, bool COLMAJOR, int TB>
+template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE = false>
 static int launch_trsv(const T* w, int64_t ldw, int n, const T* dinv, T* x, int64_t ldx, int kc, int* flags,
                        int* counter, unsigned* status, cudaStream_t stream) {
   const size_t smem = ((size_t)TB * (TB + 1) * sizeof(T) + 15) / 16 * 16 + (size_t)TB * kKC * sizeof(T);
   static bool set = false;
   if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(trsv_chain_kernel<T, LOWER, COLMAJOR, TB>,
+    RM_CUDA_TRY(cudaFuncSetAttribute(trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     set = true;
   }
   const int nblk = (n + TB - 1) / TB;
-  trsv_chain_kernel<T, LOWER, COLMAJOR, TB><<<nblk, TB * 4, smem, stream>>>(w, ldw, n, dinv, x, ldx, kc, flags, counter,
-                                                                             status);
+  trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE><<<nblk, TB * 4, smem, stream>>>(w, ldw, n, dinv, x, ldx, kc, flags,
+                                                                                  counter, status);
   RM_LAUNCHED();
   return RM_OK;
 }
@@ -302,11 +432,35 @@ int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const i
 
 // ------------------------------------------------------------------ float32, no pivoting
 
-size_t diag_blocks_f32_bytes(int64_t n) { return (size_t)((n + kTB32 - 1) / kTB32) * 2 * kTB32 * kTB32 * sizeof(float); }
+size_t diag_blocks_f32_bytes(int64_t n) {
+  return (size_t)((n + kTB32 - 1) / kTB32) * kDiagMats * kTB32 * kTB32 * sizeof(float);
+}
 
 int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream) {
   if (n == 0) return RM_OK;
   return launch_invert<float, false, kTB32>(w, ldw, n, dinv, true, false, stream);
+}
+
+int64_t premultiplied_f32_ld(int64_t n) { return (n + kTB32 - 1) / kTB32 * kTB32; }
+size_t premultiplied_f32_bytes(int64_t n) {
+  const int64_t ld = premultiplied_f32_ld(n);
+  return (size_t)ld * ld * sizeof(float);
+}
+
+int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, float* pre, cudaStream_t stream) {
+  const int nblk = (int)((n + kTB32 - 1) / kTB32);
+  if (nblk < 2) return RM_OK;
+  const size_t smem = 2 * (size_t)kTB32 * (kTB32 + 1) * sizeof(float);
+  static bool set = false;
+  if (!set) {
+    RM_CUDA_TRY(cudaFuncSetAttribute(premultiply_kernel<float, kTB32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    set = true;
+  }
+  premultiply_kernel<float, kTB32><<<nblk * nblk, 256, smem, stream>>>(lu, ld, n, dinv, pre,
+                                                                        premultiplied_f32_ld(n));
+  RM_LAUNCHED();
+  return RM_OK;
 }
 
 size_t trsv_f32_scratch_bytes(int64_t n, int64_t k) {
@@ -314,21 +468,30 @@ size_t trsv_f32_scratch_bytes(int64_t n, int64_t k) {
 }
 
 // x = U^-1 L^-1 x in place for the row-major float32 L\\U (unit L) of an LU whose row
-// permutation the caller has already applied to x.
-int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, float* x, int64_t ldx, int64_t k,
-                       void* scratch, unsigned* status, cudaStream_t stream) {
+// permutation the caller has already applied to x. With pre (premultiply_f32 of the same
+// factors; ld premultiplied_f32_ld(n)) the chains read the scaled triangles instead.
+int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, const float* pre, float* x,
+                       int64_t ldx, int64_t k, void* scratch, unsigned* status, cudaStream_t stream) {
   if (n == 0 || k == 0) return RM_OK;
   const int nblk = (int)((n + kTB32 - 1) / kTB32);
   const int chunks = (int)((k + kKC - 1) / kKC);
   int* flags = reinterpret_cast<int*>(scratch);
   RM_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)(2 * (nblk + 1)) * sizeof(int) * chunks, stream));
+  const int64_t ldp = premultiplied_f32_ld(n);
   for (int ch = 0; ch < chunks; ++ch) {
     const int kc = (int)std::min<int64_t>(kKC, k - (int64_t)ch * kKC);
     int* f = flags + (size_t)ch * 2 * (nblk + 1);
     float* xc = x + ch * kKC;
-    RM_TRY((launch_trsv<float, true, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream)));
-    RM_TRY((launch_trsv<float, false, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f + nblk + 1, f + 2 * nblk + 1,
-                                                    status, stream)));
+    if (pre) {
+      RM_TRY((launch_trsv<float, true, false, kTB32, true>(pre, ldp, (int)n, dinv, xc, ldx, kc, f, f + nblk, status,
+                                                           stream)));
+      RM_TRY((launch_trsv<float, false, false, kTB32, true>(pre, ldp, (int)n, dinv, xc, ldx, kc, f + nblk + 1,
+                                                            f + 2 * nblk + 1, status, stream)));
+    } else {
+      RM_TRY((launch_trsv<float, true, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream)));
+      RM_TRY((launch_trsv<float, false, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f + nblk + 1,
+                                                      f + 2 * nblk + 1, status, stream)));
+    }
   }
   return RM_OK;
 }

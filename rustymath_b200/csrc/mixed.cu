@@ -62,205 +62,287 @@ __global__ void to_f32_kernel(const double* __restrict__ a, int64_t lda, int64_t
 }
 
 // ------------------------------------------------------------------ the panel
+struct alignas(16) LppSlot {
+  float row[kLppLeaf];  // a warp's candidate pivot row (its current leaf columns)
+  float key;            // its |pivot|; -0.5 for NaN, -1 when the warp has no candidate
+  int idx;
+  int pad[2];
+};
+
+__device__ __forceinline__ void warp_argmax_key(float& v, int& i) {
+#pragma unroll
+  for (int off = 16; off; off >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    if (ov > v || (ov == v && oi < i)) {
+      v = ov;
+      i = oi;
+    }
+  }
+}
+
 // Factors the T x nb panel A[j0.., j0..] (T <= 256, nb <= 128) with partial pivoting among
-// its T rows: thread r owns row r for the pivot search and the rank-1 updates. Within a
-// 32-column leaf each column takes one pivot search (warp argmax, first row on ties, NaN
-// never chosen) and a rank-1 update of the leaf; after a leaf, the panel's later columns are
-// updated with a register-blocked shared-memory product. Writes the panel back, plocal[i] =
-// the panel row that row i came from, linv = L11^-1 and uinvt = (U11^-1)^T (ld 128). A zero
-// pivot sets RM_DEV_NAN and leaves its column unreduced.
-__global__ void __launch_bounds__(kLppThreads) lpp_panel_kernel(float* __restrict__ a, int64_t lda, int j0, int nb,
+// its T rows. Thread r owns row r. Pivoting is implicit: rows stay where they are and a row
+// chosen as a pivot leaves the candidates; the panel is written back in pivot order at the
+// end. Within a 32-column leaf each thread keeps its row's leaf in registers, and each
+// column costs one barrier: every warp posts its best candidate and that candidate's row, and
+// after the barrier every thread picks the winner among 8 posts (largest |pivot|, first row
+// on ties, NaN never chosen over a number) and reads the pivot row from it (two buffers of
+// posts alternate between columns, so a column's posts are never overwritten while read).
+// After a leaf: U12 of its pivot rows (unit-lower solve, a column per thread) and the block
+// update of the later columns of the rows still unchosen. Then the pivot rows come first in
+// choice order and the others follow in their original order: plocal[i] is the panel row
+// that row i came from; linv = L11^-1 and uinvt = (U11^-1)^T (ld 128). A zero pivot sets
+// RM_DEV_NAN and leaves its column unreduced.
+__global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __restrict__ a, int64_t lda, int j0, int nb,
                                                                 int T, float* __restrict__ linv,
                                                                 float* __restrict__ uinvt, int* __restrict__ plocal,
                                                                 unsigned* status) {
   extern __shared__ float sm[];
   float(*P)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm);
   float(*X)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm + kLppRows * kLppStride);
-  float(*Tm)[33] = reinterpret_cast<float(*)[33]>(sm + (kLppRows + kLppCols) * kLppStride);
-  __shared__ int perm_s[kLppRows];
-  __shared__ float red_v[kLppThreads / 32];
-  __shared__ int red_i[kLppThreads / 32];
-  __shared__ int piv_row;
+  float(*Tm)[33] = reinterpret_cast<float(*)[33]>(sm + (kLppRows + kLppCols) * kLppStride);  // 96 x 33
+  // during the factorization X's space holds the leaf's U12, transposed (column j's 32 values contiguous)
+  float(*UbT)[kLppLeaf + 4] = reinterpret_cast<float(*)[kLppLeaf + 4]>(X);
+  __shared__ LppSlot slot[2][kLppThreads / 32];
+  __shared__ __align__(16) float Lp[kLppLeaf][kLppLeaf + 4];
+  __shared__ int piv_s[kLppCols];
+  __shared__ int order_s[kLppRows];
+  __shared__ int wcount[kLppThreads / 32];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r = tid;
   float* blk = a + (int64_t)j0 * lda + j0;
-  for (int e = tid; e < kLppRows * kLppCols; e += kLppThreads) {
-    const int r = e / kLppCols, c = e % kLppCols;
-    P[r][c] = (r < T && c < nb) ? blk[(int64_t)r * lda + c] : (r == c ? 1.0f : 0.0f);
+  for (int e = tid; e < T * nb; e += kLppThreads) {
+    const int rr = e / nb, c = e % nb;
+    P[rr][c] = blk[(int64_t)rr * lda + c];
   }
-  perm_s[tid] = tid;
+  bool active = r < T;
   __syncthreads();
 
-  for (int l = 0; l < nb; l += kLppLeaf) {
-    const int lend = min(l + kLppLeaf, nb);
-    for (int c = l; c < lend; ++c) {
-      float v = (tid >= c && tid < T) ? fabsf(P[tid][c]) : -1.0f;
-      int idx = tid;
-      warp_argmax_f32(v, idx);
-      if (lane == 0) {
-        red_v[warp] = v;
-        red_i[warp] = idx;
+  for (int L = 0; L * kLppLeaf < nb; ++L) {
+    const int c0 = L * kLppLeaf;
+    const bool was_active = active;
+    float p[kLppLeaf];
+#pragma unroll
+    for (int i = 0; i < kLppLeaf; ++i) p[i] = (active && c0 + i < nb) ? P[r][c0 + i] : 0.0f;
+#pragma unroll
+    for (int c = 0; c < kLppLeaf; ++c) {
+      if (c0 + c >= nb) continue;  // the last panel may be narrower than a leaf
+      LppSlot* sl = &slot[c & 1][0];
+      float key = -1.0f;
+      if (active) {
+        const float v = fabsf(p[c]);
+        key = v != v ? -0.5f : v;
+      }
+      int idx = r;
+      warp_argmax_key(key, idx);
+      if (lane == (idx & 31)) {  // the warp's candidate (any lane when the warp has none)
+        float4* dst = reinterpret_cast<float4*>(sl[warp].row);
+#pragma unroll
+        for (int i = 0; i < kLppLeaf / 4; ++i) dst[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
+        sl[warp].key = key;
+        sl[warp].idx = idx;
       }
       __syncthreads();
-      if (warp == 0) {
-        v = lane < kLppThreads / 32 ? red_v[lane] : -1.0f;
-        idx = lane < kLppThreads / 32 ? red_i[lane] : INT_MAX;
-        warp_argmax_f32(v, idx);
-        if (lane == 0) piv_row = v < 0.0f ? c : idx;  // every candidate NaN: keep the diagonal
-      }
-      __syncthreads();
-      const int p = piv_row;
-      if (p != c) {
-        if (tid < kLppCols) {
-          const float t = P[c][tid];
-          P[c][tid] = P[p][tid];
-          P[p][tid] = t;
+      float bk = sl[0].key;
+      int bi = sl[0].idx, bw = 0;
+#pragma unroll
+      for (int w = 1; w < kLppThreads / 32; ++w) {
+        const float k2 = sl[w].key;
+        const int i2 = sl[w].idx;
+        if (k2 > bk || (k2 == bk && i2 < bi)) {
+          bk = k2;
+          bi = i2;
+          bw = w;
         }
-        if (tid == 0) {
-          const int t = perm_s[c];
-          perm_s[c] = perm_s[p];
-          perm_s[p] = t;
+      }
+      // the pivot row, as 16-byte reads of the winning post
+      float prow[kLppLeaf];
+      {
+        const float4* src = reinterpret_cast<const float4*>(sl[bw].row);
+#pragma unroll
+        for (int i = c / 4; i < kLppLeaf / 4; ++i) {
+          const float4 v4 = src[i];
+          prow[4 * i] = v4.x, prow[4 * i + 1] = v4.y, prow[4 * i + 2] = v4.z, prow[4 * i + 3] = v4.w;
         }
       }
-      __syncthreads();
-      const float piv = P[c][c];
-      if (piv != 0.0f) {
-        if (tid > c && tid < T) {
-          const float lv = P[tid][c] * (1.0f / piv);
-          P[tid][c] = lv;
-          for (int cc = c + 1; cc < lend; ++cc) P[tid][cc] = fmaf(-lv, P[c][cc], P[tid][cc]);
+      const float piv = prow[c];
+      if (warp == (bi >> 5)) {  // warp-uniform: only the pivot's warp records it
+        if (r == bi) {
+          active = false;
+          piv_s[c0 + c] = r;
+          float4* dst = reinterpret_cast<float4*>(Lp[c]);
+#pragma unroll
+          for (int i = 0; i < kLppLeaf / 4; ++i) dst[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
         }
-      } else if (tid == 0) {
-        flag_error(status, RM_DEV_NAN);
       }
-      __syncthreads();
+      if (active && piv != 0.0f) {
+        const float l = p[c] * __frcp_rn(piv);
+        p[c] = l;
+#pragma unroll
+        for (int i = c + 1; i < kLppLeaf; ++i) p[i] = fmaf(-l, prow[i], p[i]);
+      }
+      if (piv == 0.0f && tid == 0) flag_error(status, RM_DEV_NAN);
     }
-    if (lend < nb) {
-      // rows l..lend-1 of the later columns: substitution with the leaf's unit lower block
-      for (int cc = lend + tid; cc < nb; cc += kLppThreads)
-        for (int i = l + 1; i < lend; ++i) {
-          float s = P[i][cc];
-          for (int q = l; q < i; ++q) s = fmaf(-P[i][q], P[q][cc], s);
-          P[i][cc] = s;
-        }
-      __syncthreads();
-      // rows lend..T-1 of the later columns -= L(rows, leaf) U(leaf, columns)
-      const int ty = tid >> 4, tx = tid & 15;
-      constexpr int RI = kLppRows / 16, CJ = kLppCols / 16;
-      float acc[RI][CJ];
+    if (was_active) {
 #pragma unroll
-      for (int i = 0; i < RI; ++i)
-#pragma unroll
-        for (int j = 0; j < CJ; ++j) acc[i][j] = 0.0f;
-      for (int q = l; q < lend; ++q) {
-        float rv[RI], cv[CJ];
-#pragma unroll
-        for (int i = 0; i < RI; ++i) {
-          const int r = lend + ty + 16 * i;
-          rv[i] = r < T ? P[r][q] : 0.0f;
-        }
-#pragma unroll
-        for (int j = 0; j < CJ; ++j) {
-          const int cc = lend + tx + 16 * j;
-          cv[j] = cc < nb ? P[q][cc] : 0.0f;
-        }
-#pragma unroll
-        for (int i = 0; i < RI; ++i)
-#pragma unroll
-          for (int j = 0; j < CJ; ++j) acc[i][j] = fmaf(rv[i], cv[j], acc[i][j]);
-      }
-#pragma unroll
-      for (int i = 0; i < RI; ++i)
-#pragma unroll
-        for (int j = 0; j < CJ; ++j) {
-          const int r = lend + ty + 16 * i, cc = lend + tx + 16 * j;
-          if (r < T && cc < nb) P[r][cc] -= acc[i][j];
-        }
-      __syncthreads();
+      for (int i = 0; i < kLppLeaf; ++i)
+        if (c0 + i < nb) P[r][c0 + i] = p[i];
     }
+    __syncthreads();
+    const int rc0 = c0 + kLppLeaf, rcols = nb - rc0;
+    if (rcols <= 0) break;
+    // U12 of the leaf's pivot rows: u = Lp^-1 (their later columns), a column per thread
+    if (tid < rcols) {  // rcols < 128 <= threads
+      const int j = tid;
+      float u[kLppLeaf];
+#pragma unroll
+      for (int c = 0; c < kLppLeaf; ++c) u[c] = P[piv_s[c0 + c]][rc0 + j];
+#pragma unroll
+      for (int c = 1; c < kLppLeaf; ++c)
+#pragma unroll
+        for (int q = 0; q < c; ++q) u[c] = fmaf(-Lp[c][q], u[q], u[c]);
+#pragma unroll
+      for (int c = 0; c < kLppLeaf; ++c) {
+        P[piv_s[c0 + c]][rc0 + j] = u[c];
+        UbT[j][c] = u[c];
+      }
+    }
+    __syncthreads();
+    // the rows still unchosen: later columns -= L(row, leaf) U12
+    if (active) {
+      for (int j = 0; j < rcols; ++j) {
+        float acc = P[r][rc0 + j];
+        const float4* ub = reinterpret_cast<const float4*>(&UbT[j][0]);
+#pragma unroll
+        for (int q = 0; q < kLppLeaf / 4; ++q) {
+          const float4 u4 = ub[q];
+          acc = fmaf(-p[4 * q], u4.x, acc);
+          acc = fmaf(-p[4 * q + 1], u4.y, acc);
+          acc = fmaf(-p[4 * q + 2], u4.z, acc);
+          acc = fmaf(-p[4 * q + 3], u4.w, acc);
+        }
+        P[r][rc0 + j] = acc;
+      }
+    }
+    __syncthreads();
   }
-  for (int e = tid; e < T * nb; e += kLppThreads) {
-    const int r = e / nb, c = e % nb;
-    blk[(int64_t)r * lda + c] = P[r][c];
-  }
-  if (tid < T) plocal[tid] = perm_s[tid];
 
-  // ---- L11^-1 (unit lower) into X: 32x32 diagonal blocks by column substitution (a warp
-  // each, a lane per column), the blocks below them in order of distance from the diagonal
-  for (int e = tid; e < kLppCols * kLppCols; e += kLppThreads) X[e / kLppCols][e % kLppCols] = 0.0f;
+  // the row order: pivot rows in choice order, then the unchosen rows in their own order
+  const bool rest = active;  // r < T and never chosen
+  const unsigned msk = __ballot_sync(0xffffffffu, rest);
+  if (lane == 0) wcount[warp] = __popc(msk);
+  if (tid < nb) order_s[tid] = piv_s[tid];
+  __syncthreads();
+  if (rest) {
+    int before = nb;
+    for (int w = 0; w < warp; ++w) before += wcount[w];
+    order_s[before + __popc(msk & ((1u << lane) - 1u))] = r;
+  }
+  __syncthreads();
+  if (tid < T) plocal[tid] = order_s[tid];
+  // the panel back in that order: a warp per row, lanes along it
+  for (int rr = warp; rr < T; rr += kLppThreads / 32) {
+    const float* src = P[order_s[rr]];
+    float* dst = blk + (int64_t)rr * lda;
+    for (int c = lane; c < nb; c += 32) dst[c] = src[c];
+  }
+  // ---- the inverses. D (P's rows 0..127) = the diagonal block in pivot order: L11 below its
+  // diagonal (unit), U11 on and above it. XL (X's space) = L11^-1 and XU (P's rows 128..) =
+  // (U11^T)^-1 = (U11^-1)^T are both lower triangles, built the same way: the diagonal 32 x 32
+  // blocks first (a warp each, a lane per column, zeros above their diagonals), then the
+  // blocks below in order of distance b - a = gap: T = sum_{c=a..b-1} M_bc X_ca in Tm,
+  // X_ba = -X_bb T, each thread a 2 x 2 piece of every block of a gap. M_0(i, k) = D[i][k],
+  // M_1(i, k) = D[k][i].
+  float(*D)[kLppStride] = P;
+  float(*XL)[kLppStride] = X;
+  float(*XU)[kLppStride] = P + kLppCols;
+  for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32) {
+    const float* src = P[rr < nb ? order_s[rr] : 0];
+    for (int c = lane; c < kLppCols; c += 32) X[rr][c] = (rr < nb && c < nb) ? src[c] : (rr == c ? 1.0f : 0.0f);
+  }
+  __syncthreads();
+  for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32)
+    for (int c = lane; c < kLppCols; c += 32) D[rr][c] = X[rr][c];
   __syncthreads();
   if (warp < 4) {
     const int b0 = warp * 32;
     float x[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
-      float s = i == lane ? 1.0f : 0.0f;
+      float acc = i == lane ? 1.0f : 0.0f;
 #pragma unroll
-      for (int k2 = 0; k2 < i; ++k2) s = fmaf(-P[b0 + i][b0 + k2], x[k2], s);
-      x[i] = i < lane ? 0.0f : s;
+      for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + i][b0 + k2], x[k2], acc);
+      x[i] = i < lane ? 0.0f : acc;
     }
 #pragma unroll
-    for (int i = 0; i < 32; ++i) X[b0 + i][b0 + lane] = x[i];
-  }
-  __syncthreads();
-  for (int gap = 1; gap < 4; ++gap)
-    for (int ab = 0; ab + gap < 4; ++ab) {
-      const int rb = (ab + gap) * 32, ca = ab * 32;
-      for (int e = tid; e < 1024; e += kLppThreads) {  // Tm = sum_{c=a..b-1} L_bc X_ca
-        const int i = e >> 5, j = e & 31;
-        float s = 0.0f;
-        for (int k2 = ca; k2 < rb; ++k2) s = fmaf(P[rb + i][k2], X[k2][ca + j], s);
-        Tm[i][j] = s;
-      }
-      __syncthreads();
-      for (int e = tid; e < 1024; e += kLppThreads) {  // X_ba = -D_b^-1 Tm
-        const int i = e >> 5, j = e & 31;
-        float s = 0.0f;
-        for (int k2 = 0; k2 <= i; ++k2) s = fmaf(X[rb + i][rb + k2], Tm[k2][j], s);
-        X[rb + i][ca + j] = -s;
-      }
-      __syncthreads();
-    }
-  for (int e = tid; e < kLppCols * kLppCols; e += kLppThreads) linv[e] = X[e / kLppCols][e % kLppCols];
-  __syncthreads();
-  // ---- U11^-1 (upper) into X, written transposed
-  for (int e = tid; e < kLppCols * kLppCols; e += kLppThreads) X[e / kLppCols][e % kLppCols] = 0.0f;
-  __syncthreads();
-  if (warp < 4) {
-    const int b0 = warp * 32;
+    for (int i = 0; i < 32; ++i) XL[b0 + i][b0 + lane] = x[i];
+  } else {
+    const int b0 = (warp - 4) * 32;
     float x[32];
 #pragma unroll
-    for (int i = 31; i >= 0; --i) {
-      float s = i == lane ? 1.0f : 0.0f;
+    for (int i = 0; i < 32; ++i) {
+      float acc = i == lane ? 1.0f : 0.0f;
 #pragma unroll
-      for (int k2 = i + 1; k2 < 32; ++k2) s = fmaf(-P[b0 + i][b0 + k2], x[k2], s);
-      x[i] = i > lane ? 0.0f : s / P[b0 + i][b0 + i];
+      for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + k2][b0 + i], x[k2], acc);
+      x[i] = i < lane ? 0.0f : acc / D[b0 + i][b0 + i];
     }
 #pragma unroll
-    for (int i = 0; i < 32; ++i) X[b0 + i][b0 + lane] = x[i];
+    for (int i = 0; i < 32; ++i) XU[b0 + i][b0 + lane] = x[i];
   }
   __syncthreads();
-  for (int gap = 1; gap < 4; ++gap)
-    for (int ab = 0; ab + gap < 4; ++ab) {
-      const int ra = ab * 32, cb = (ab + gap) * 32;
-      for (int e = tid; e < 1024; e += kLppThreads) {  // Tm = sum_{c=a+1..b} U_ac X_cb
-        const int i = e >> 5, j = e & 31;
-        float s = 0.0f;
-        for (int k2 = ra + 32; k2 < cb + 32; ++k2) s = fmaf(P[ra + i][k2], X[k2][cb + j], s);
-        Tm[i][j] = s;
+  {
+    const int ti = tid >> 4, tj = tid & 15;  // rows ti, ti+16 and columns tj, tj+16 of a block
+    float(*Tq)[33] = Tm;                     // up to 3 blocks of 32 x 33
+    for (int gap = 1; gap < 4; ++gap)
+      for (int m = 0; m < 2; ++m) {
+        float(*Xm)[kLppStride] = m == 0 ? XL : XU;
+        for (int a = 0; a + gap < 4; ++a) {
+          const int b = a + gap;
+          float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
+          const int r0 = 32 * b + ti, r1 = r0 + 16, c0 = 32 * a + tj, c1 = c0 + 16;
+          if (m == 0) {
+#pragma unroll 4
+            for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
+              const float m0 = D[r0][k2], m1 = D[r1][k2], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
+              t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
+            }
+          } else {
+#pragma unroll 4
+            for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
+              const float m0 = D[k2][r0], m1 = D[k2][r1], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
+              t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
+            }
+          }
+          float(*T1)[33] = Tq + 32 * a;
+          T1[ti][tj] = t00, T1[ti][tj + 16] = t01, T1[ti + 16][tj] = t10, T1[ti + 16][tj + 16] = t11;
+        }
+        __syncthreads();
+        for (int a = 0; a + gap < 4; ++a) {
+          const int b = a + gap;
+          float(*T1)[33] = Tq + 32 * a;
+          float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
+          const int r0 = 32 * b + ti, r1 = r0 + 16;
+#pragma unroll 4
+          for (int k2 = 0; k2 < 32; ++k2) {
+            const float x0 = Xm[r0][32 * b + k2], x1 = Xm[r1][32 * b + k2];
+            const float u0 = T1[k2][tj], u1 = T1[k2][tj + 16];
+            t00 = fmaf(x0, u0, t00), t01 = fmaf(x0, u1, t01), t10 = fmaf(x1, u0, t10), t11 = fmaf(x1, u1, t11);
+          }
+          Xm[r0][32 * a + tj] = -t00, Xm[r0][32 * a + tj + 16] = -t01, Xm[r1][32 * a + tj] = -t10,
+                          Xm[r1][32 * a + tj + 16] = -t11;
+        }
+        __syncthreads();
       }
-      __syncthreads();
-      for (int e = tid; e < 1024; e += kLppThreads) {  // X_ab = -D_a^-1 Tm
-        const int i = e >> 5, j = e & 31;
-        float s = 0.0f;
-        for (int k2 = i; k2 < 32; ++k2) s = fmaf(X[ra + i][ra + k2], Tm[k2][j], s);
-        X[ra + i][cb + j] = -s;
-      }
-      __syncthreads();
+  }
+  for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32)
+    for (int c = lane; c < kLppCols; c += 32) {
+      linv[rr * kLppCols + c] = rr >= c ? XL[rr][c] : 0.0f;
+      uinvt[rr * kLppCols + c] = rr >= c ? XU[rr][c] : 0.0f;
     }
-  for (int e = tid; e < kLppCols * kLppCols; e += kLppThreads) uinvt[e] = X[e % kLppCols][e / kLppCols];
 }
 
-constexpr size_t kLppSmem = ((size_t)(kLppRows + kLppCols) * kLppStride + 32 * 33) * sizeof(float);
+constexpr size_t kLppSmem = ((size_t)(kLppRows + kLppCols) * kLppStride + 3 * 32 * 33) * sizeof(float);
 
 // ------------------------------------------------------------------ the panel's row permutation
 constexpr int kApplyCols = 32;

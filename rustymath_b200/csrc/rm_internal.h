@@ -48,8 +48,11 @@ int regular_flag_f64(const double* w, int64_t ldw, int64_t n, const double* amax
 // ---------------------------------------------------------------- solves (getrs.cu)
 constexpr int kSolveBlock = 64;  // rows of a block row of the triangular solves
 constexpr int kSolveCols = 16;   // right-hand-side columns per solve launch
+// Per block row of a triangular solve: the inverses of its two diagonal blocks (L, U) and
+// the two couplings to the block solved just before it (inverse x off-diagonal block).
+constexpr int kDiagMats = 4;
 constexpr size_t diag_blocks_bytes_max(int64_t n) {
-  return (size_t)((n + kSolveBlock - 1) / kSolveBlock) * 2 * kSolveBlock * kSolveBlock * sizeof(double);
+  return (size_t)((n + kSolveBlock - 1) / kSolveBlock) * kDiagMats * kSolveBlock * kSolveBlock * sizeof(double);
 }
 constexpr size_t getrs_scratch_bytes_max(int64_t n, int64_t k) {
   return ((size_t)n * k * sizeof(double) + 255) / 256 * 256 +
@@ -113,8 +116,11 @@ int accumulate_f64(const float* c, int64_t ldc, int64_t n, int64_t k, double* x,
 size_t diag_blocks_f32_bytes(int64_t n);
 int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream);
 size_t trsv_f32_scratch_bytes(int64_t n, int64_t k);
-int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, float* x, int64_t ldx, int64_t k,
-                       void* scratch, unsigned* status, cudaStream_t stream);
+int64_t premultiplied_f32_ld(int64_t n);
+size_t premultiplied_f32_bytes(int64_t n);
+int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, float* pre, cudaStream_t stream);
+int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, const float* pre, float* x,
+                       int64_t ldx, int64_t k, void* scratch, unsigned* status, cudaStream_t stream);
 
 // ---------------------------------------------------------------- helpers (api.cu)
 int64_t round_up(int64_t x, int64_t m);
