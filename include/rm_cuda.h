@@ -134,6 +134,52 @@ int rm_dsolve(int64_t n, const double *d_a, const double *d_b, int64_t k, double
 int rm_dsolve_host(int64_t n, const double *h_a, const double *h_b, int64_t k, double *h_x,
                    const rm_solve_options *opts, rm_solve_report *report);
 
+/* ---- Batched solves: many small systems of uneven size in one persistent launch.
+ * System i is the n[i] x n[i] row-major float64 A at d_a + a_off[i] (items), its right-hand
+ * sides the n[i] x k[i] row-major d_b + b_off[i], its solution d_x + x_off[i]; 0 <= n[i] <= 256
+ * and 0 <= k[i] <= 8. rustymath solves a stack of same-size systems one LuWork per thread
+ * (Stacked::solve, src/linalg/stacked.rs:88-101, each factor.rs:207-209); these entry points
+ * take uneven sizes, which a rustymath stack cannot hold. opts->method picks float32 factors
+ * + float64 refinement (RM_METHOD_F32_IR, with per-system fallback to float64 when
+ * opts->fallback) or float64 factors (RM_METHOD_PLAIN_F64); every system's normwise backward
+ * error is measured in float64. A plan holds the sorted order, the scratch and a CUDA graph
+ * of the launch; rm_batch_plan_tune picks the panel width of each size bucket by timing. */
+typedef struct rm_batch_report {
+  double max_backward_error; /* over the systems (NaN if any is NaN) */
+  int64_t fell_back;         /* systems answered by the float64 fallback */
+  int64_t not_regular;       /* systems whose float64 factors fail rustymath's regular test */
+  int64_t no_convergence;    /* systems left unrefined (fallback off) */
+  int32_t max_iterations;    /* most refinement steps any system took */
+} rm_batch_report;
+
+/* per-system flags from rm_batch_plan_results */
+#define RM_BATCH_FELL_BACK 1
+#define RM_BATCH_NOT_REGULAR 2
+#define RM_BATCH_NO_CONVERGENCE 4
+
+typedef struct rm_batch_plan rm_batch_plan;
+int rm_batch_plan_create(int64_t count, const int64_t *h_n, const int64_t *h_k, const int64_t *h_a_off,
+                         const int64_t *h_b_off, const int64_t *h_x_off, const rm_solve_options *opts,
+                         rm_batch_plan **plan);
+/* Times each size bucket's candidate panel widths on these inputs (solving them) and keeps the
+ * fastest; synchronises on `stream`. */
+int rm_batch_plan_tune(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x, void *stream);
+/* One persistent kernel launch for all systems, replayed from a CUDA graph; asynchronous on
+ * `stream`. */
+int rm_batch_plan_execute(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x, void *stream);
+/* Per-system backward errors, refinement steps and RM_BATCH_* flags of the last execute (any
+ * pointer may be NULL); synchronises. */
+int rm_batch_plan_results(rm_batch_plan *plan, double *h_berr, int32_t *h_iters, int32_t *h_flags,
+                          rm_batch_report *summary);
+/* The panel width chosen for size bucket 0..4 (n <= 32, 64, 128, 192, 256). */
+int rm_batch_plan_panel_width(const rm_batch_plan *plan, int bucket);
+int rm_batch_plan_destroy(rm_batch_plan *plan);
+/* create + execute + results + destroy; synchronises. RM_NO_CONVERGENCE when a system stalled
+ * with fallback off. */
+int rm_dsolve_batched(int64_t count, const int64_t *h_n, const int64_t *h_k, const int64_t *h_a_off,
+                      const int64_t *h_b_off, const int64_t *h_x_off, const double *d_a, const double *d_b,
+                      double *d_x, const rm_solve_options *opts, rm_batch_report *report, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

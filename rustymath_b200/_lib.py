@@ -25,6 +25,14 @@ class SolveReport(ctypes.Structure):
                 ("regular", _i32)]
 
 
+class BatchReport(ctypes.Structure):
+    _fields_ = [("max_backward_error", _f64), ("fell_back", _i64), ("not_regular", _i64),
+                ("no_convergence", _i64), ("max_iterations", _i32)]
+
+
+RM_BATCH_FELL_BACK, RM_BATCH_NOT_REGULAR, RM_BATCH_NO_CONVERGENCE = 1, 2, 4
+
+
 # name -> (restype, argtypes); the set of exported entry points the header declares.
 SIGNATURES = {
     "rm_version": (ctypes.c_int, []),
@@ -47,6 +55,15 @@ SIGNATURES = {
                                  _p]),
     "rm_dsolve_host": (ctypes.c_int, [_i64, _p, _p, _i64, _p, ctypes.POINTER(SolveOptions),
                                       ctypes.POINTER(SolveReport)]),
+    "rm_batch_plan_create": (ctypes.c_int, [_i64, _p, _p, _p, _p, _p, ctypes.POINTER(SolveOptions),
+                                            ctypes.POINTER(_p)]),
+    "rm_batch_plan_tune": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "rm_batch_plan_execute": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "rm_batch_plan_results": (ctypes.c_int, [_p, _p, _p, _p, ctypes.POINTER(BatchReport)]),
+    "rm_batch_plan_panel_width": (ctypes.c_int, [_p, ctypes.c_int]),
+    "rm_batch_plan_destroy": (ctypes.c_int, [_p]),
+    "rm_dsolve_batched": (ctypes.c_int, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.POINTER(SolveOptions),
+                                         ctypes.POINTER(BatchReport), _p]),
 }
 
 

@@ -220,7 +220,7 @@ static LuBuffers plan_lu(Arena& arena, int64_t n) {
 
 static cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-static int check_device() {
+int check_device() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {

@@ -1,0 +1,858 @@
+// Batched solves of many small systems of uneven size (n <= 256, k <= 8) in one persistent
+// launch: float32 LU with partial pivoting + float64 refinement per system, falling back to a
+// float64 LU for the systems whose refinement stalls, all inside the same kernel.
+//
+// rustymath solves a stack of systems one LuWork per thread (Stacked::solve,
+// src/linalg/stacked.rs:88-101, over parallel::stack, core/src/parallel.rs:118-192), each an
+// lu_factor + lu_solve (core/src/linalg/factor.rs:617-641) and, when `regular` fails
+// (factor.rs:221-226), least squares. Here a CTA takes one system at a time from a shared
+// counter (systems sorted by size, largest first, so the long ones start early) and:
+//   - loads A (float64, row-major) into a float32 working copy W in its own slice of a global
+//     scratch (W stays in L2 while the CTA works on it); thread r owns row r;
+//   - factors W with partial pivoting, implicitly: rows never move, a row chosen as pivot of
+//     logical column c records pos = c and leaves the candidates; in panels of NB columns
+//     (16 or 32, picked per size bucket by the tuner) each thread keeps its row's panel in
+//     registers and each column costs one barrier (every warp posts its best candidate row,
+//     every thread picks the winner among the posts: largest |pivot|, lowest row on ties, NaN
+//     never chosen over a number); then U12 of the panel's pivot rows (a column per thread)
+//     and the update of the rows not chosen yet;
+//   - solves L U x = P b with the rows' right-hand sides in registers, block by block (a warp
+//     solves each NB x NB diagonal block with shuffles);
+//   - refines in float64: r = b - A x (a warp per row of A, x in shared memory), the normwise
+//     backward error max_c ||r_c|| / (||A|| ||x_c|| + ||b_c||), and corrections from the
+//     float32 factors until it is at most the tolerance (n * 2^-53 by default);
+//   - on a stall (the error not halving) or the step limit, redoes the system in float64
+//     (the same code on float64 items, reusing the slice) and reports the fallback; a pivot
+//     at most eps * n * max|a| there marks the system not regular, as rustymath's `regular`.
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <numeric>
+#include <vector>
+
+#include "rm_internal.h"
+
+namespace rm {
+namespace bt {
+
+constexpr int THREADS = 256;
+constexpr int WARPS = THREADS / 32;
+constexpr int NMAX = 256;  // rows of a system: a thread per row
+constexpr int KMAX = 8;    // right-hand sides of a system
+constexpr int SLOT_BYTES = 144;
+constexpr int UBT_BYTES = NMAX * 20 * 8;  // U12 transposed: NMAX x (NB + 4) items, either type
+
+// result flags per system
+constexpr int FLAG_FELL_BACK = 1;
+constexpr int FLAG_NOT_REGULAR = 2;
+constexpr int FLAG_NO_CONVERGENCE = 4;
+
+struct Smem {
+  alignas(16) unsigned char slot[2][WARPS][SLOT_BYTES];  // posts: NB items, then key (T), row
+  alignas(16) unsigned char lp[32 * 36 * 4];              // the panel's pivot rows (NB x (NB + 4) items)
+  alignas(16) unsigned char ubt[UBT_BYTES];               // U12 of a panel, transposed
+  alignas(16) double xs[NMAX][KMAX];                      // the float64 solution, by unknown
+  alignas(16) double rs[NMAX][KMAX];                      // the float64 residual, by row
+  alignas(16) double vsm[32][KMAX];                       // a diagonal block's right-hand sides
+  int piv[NMAX];                                          // logical position -> row
+  double red[WARPS][3 * KMAX + 1];
+  double anorm, bnorm[KMAX];
+  int zero_pivot;
+};
+
+template <typename T>
+__device__ __forceinline__ T tabs(T v) {
+  return v < T(0) ? -v : v;
+}
+
+// rustymath's divide: multiply by the reciprocal unless the pivot is subnormal
+__device__ __forceinline__ double bdivide(double x, double piv) {
+  return fabs(piv) < DBL_MIN ? x / piv : x * (1.0 / piv);
+}
+__device__ __forceinline__ float bdivide(float x, float piv) {
+  return fabsf(piv) < FLT_MIN ? x / piv : x * __frcp_rn(piv);
+}
+
+template <typename T>
+__device__ __forceinline__ void warp_argmax(T& v, int& i) {
+#pragma unroll
+  for (int off = 16; off; off >>= 1) {
+    const T ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    if (ov > v || (ov == v && oi < i)) {
+      v = ov;
+      i = oi;
+    }
+  }
+}
+
+// Loads the n x n row-major float64 a into W (row-major, ld), converted to T: a warp per
+// row, lanes along it.
+template <typename T>
+__device__ void load_w(const double* __restrict__ a, int n, T* W, int ld) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = warp; r < n; r += WARPS)
+    for (int j = lane; j < n; j += 32) W[(int64_t)r * ld + j] = (T)__ldcs(a + (int64_t)r * n + j);
+}
+
+// Implicitly pivoted LU of the n x n W (row-major, ld): thread r owns row r; my_pos (in/out)
+// is the logical position of row r, -1 before it is chosen; sm.piv[c] is the row chosen for
+// column c. Returns with every thread's my_pos set. A zero pivot sets sm.zero_pivot and
+// leaves its column unreduced.
+template <typename T, int NB>
+__device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r = tid;
+  T(*Lp)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(sm.lp);
+  T(*UbT)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(sm.ubt);
+  bool active = r < n;
+  my_pos = -1;
+  for (int J = 0; J < n; J += NB) {
+    const int nbj = min(NB, n - J);
+    const bool was_active = active;
+    T p[NB];
+    T* row = W + (int64_t)r * ld + J;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = (active && i < nbj) ? row[i] : T(0);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+      if (c < nbj) {
+        unsigned char(*sl)[SLOT_BYTES] = sm.slot[c & 1];
+        T key = T(-1);
+        if (active) {
+          const T v = tabs(p[c]);
+          key = v != v ? T(-0.5) : v;
+        }
+        int idx = r;
+        warp_argmax(key, idx);
+        if (lane == (idx & 31)) {
+          T* post = reinterpret_cast<T*>(sl[warp]);
+#pragma unroll
+          for (int i = 0; i < NB; ++i) post[i] = p[i];
+          *reinterpret_cast<T*>(sl[warp] + 128) = key;
+          *reinterpret_cast<int*>(sl[warp] + 136) = idx;
+        }
+        __syncthreads();
+        T bk = *reinterpret_cast<const T*>(sl[0] + 128);
+        int bi = *reinterpret_cast<const int*>(sl[0] + 136), bw = 0;
+#pragma unroll
+        for (int w = 1; w < WARPS; ++w) {
+          const T k2 = *reinterpret_cast<const T*>(sl[w] + 128);
+          const int i2 = *reinterpret_cast<const int*>(sl[w] + 136);
+          if (k2 > bk || (k2 == bk && i2 < bi)) {
+            bk = k2;
+            bi = i2;
+            bw = w;
+          }
+        }
+        const T* prow = reinterpret_cast<const T*>(sl[bw]);
+        const T piv = prow[c];
+        if (warp == (bi >> 5)) {
+          if (r == bi) {
+            active = false;
+            my_pos = J + c;
+            sm.piv[J + c] = r;
+#pragma unroll
+            for (int i = 0; i < NB; ++i) Lp[c][i] = p[i];
+          }
+        }
+        if (active) {
+          if (piv != T(0)) {
+            const T l = bdivide(p[c], piv);
+            p[c] = l;
+#pragma unroll
+            for (int i = c + 1; i < NB; ++i) p[i] = fma(-l, prow[i], p[i]);
+          }
+        }
+        if (piv == T(0) && tid == 0) sm.zero_pivot = 1;
+      }
+    }
+    if (was_active) {
+#pragma unroll
+      for (int i = 0; i < NB; ++i)
+        if (i < nbj) row[i] = p[i];
+    }
+    __syncthreads();
+    const int rc0 = J + nbj, rcols = n - rc0;
+    if (rcols > 0) {
+      // U12 of the panel's pivot rows: u = Lp^-1 (their later columns), a column per thread
+      for (int j = tid; j < rcols; j += THREADS) {
+        T u[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) u[c] = c < nbj ? W[(int64_t)sm.piv[J + c] * ld + rc0 + j] : T(0);
+#pragma unroll
+        for (int c = 1; c < NB; ++c)
+#pragma unroll
+          for (int q = 0; q < c; ++q) u[c] = fma(-Lp[c][q], u[q], u[c]);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+          if (c < nbj) W[(int64_t)sm.piv[J + c] * ld + rc0 + j] = u[c];
+          UbT[j][c] = u[c];
+        }
+      }
+      __syncthreads();
+      // the rows not chosen yet: later columns -= L(row, panel) U12
+      if (active) {
+        T* rrow = W + (int64_t)r * ld + rc0;
+        for (int j = 0; j < rcols; ++j) {
+          T acc = rrow[j];
+#pragma unroll
+          for (int c = 0; c < NB; ++c) acc = fma(-p[c], UbT[j][c], acc);
+          rrow[j] = acc;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Solves L U x = P v: thread r holds v (its row's k right-hand sides) on entry and x[my_pos]
+// on return. W holds the implicitly pivoted factors of bfactor<T, NB>.
+template <typename T, int NB>
+__device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T (&v)[KMAX]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r = tid;
+  const T* row = W + (int64_t)r * ld;
+  // forward: blocks of NB logical columns
+  for (int J = 0; J < n; J += NB) {
+    const int nbj = min(NB, n - J);
+    if (my_pos >= J && my_pos < J + nbj)
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
+    __syncthreads();
+    if (warp == 0) {
+      T y[KMAX], lrow[NB];
+      const T* prow = W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J;
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) lrow[q] = (lane < nbj && q < lane) ? prow[q] : T(0);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        if (q < nbj) {
+#pragma unroll
+          for (int c = 0; c < KMAX; ++c) {
+            const T yq = __shfl_sync(0xffffffffu, y[c], q);
+            if (lane > q) y[c] = fma(-lrow[q], yq, y[c]);
+          }
+        }
+      }
+      if (lane < nbj)
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+    }
+    __syncthreads();
+    if (r < n) {
+      if (my_pos >= J + nbj) {
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+          if (q < nbj) {
+            const T l = row[J + q];
+#pragma unroll
+            for (int c = 0; c < KMAX; ++c) v[c] = fma(-l, (T)sm.vsm[q][c], v[c]);
+          }
+      } else if (my_pos >= J) {
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
+      }
+    }
+    __syncthreads();
+  }
+  // backward
+  const int last = (n - 1) / NB * NB;
+  for (int J = last; J >= 0; J -= NB) {
+    const int nbj = min(NB, n - J);
+    if (my_pos >= J && my_pos < J + nbj)
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
+    __syncthreads();
+    if (warp == 0) {
+      T y[KMAX], urow[NB];
+      const T* prow = W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J;
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) urow[q] = (lane < nbj && q >= lane && q < nbj) ? prow[q] : T(0);
+#pragma unroll
+      for (int q = NB - 1; q >= 0; --q) {
+        if (q < nbj) {
+#pragma unroll
+          for (int c = 0; c < KMAX; ++c) {
+            if (lane == q) y[c] = y[c] / urow[q];
+            const T xq = __shfl_sync(0xffffffffu, y[c], q);
+            if (lane < q) y[c] = fma(-urow[q], xq, y[c]);
+          }
+        }
+      }
+      if (lane < nbj)
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+    }
+    __syncthreads();
+    if (r < n) {
+      if (my_pos >= 0 && my_pos < J) {
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+          if (q < nbj) {
+            const T u = row[J + q];
+#pragma unroll
+            for (int c = 0; c < KMAX; ++c) v[c] = fma(-u, (T)sm.vsm[q][c], v[c]);
+          }
+      } else if (my_pos >= J && my_pos < J + nbj) {
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// sm.rs = b - A sm.xs for the n x n row-major a (a warp per row, lanes along it) and returns
+// the normwise backward error (NaN if a residual is NaN). The first call (sm.anorm < 0)
+// also forms ||A||_inf and ||b_c||_inf.
+__device__ double bresidual(const double* __restrict__ a, const double* __restrict__ b, int n, int k, Smem& sm) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool first = sm.anorm < 0.0;
+  double rmax[KMAX], bmax[KMAX], xmax[KMAX], amax = 0.0;
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c) {
+    rmax[c] = bmax[c] = 0.0;
+    xmax[c] = tid < n ? fabs(sm.xs[tid][c]) : 0.0;
+  }
+  for (int r = warp; r < n; r += WARPS) {
+    const double* ar = a + (int64_t)r * n;
+    double acc[KMAX], asum = 0.0;
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) acc[c] = 0.0;
+    for (int j = lane; j < n; j += 32) {
+      const double av = __ldg(ar + j);
+      asum += fabs(av);
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) acc[c] = fma(av, sm.xs[j][c], acc[c]);
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+      asum += __shfl_xor_sync(0xffffffffu, asum, off);
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+    }
+    amax = fmax(amax, asum);
+    if (lane < k) {
+      double mine = 0.0;
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c)
+        if (c == lane) mine = acc[c];
+      const double bv = b[(int64_t)r * k + lane];
+      const double rv = bv - mine;
+      sm.rs[r][lane] = rv;
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c)
+        if (c == lane) {
+          rmax[c] = (fabs(rv) > rmax[c] || rv != rv) ? fabs(rv) : rmax[c];
+          bmax[c] = fmax(bmax[c], fabs(bv));
+        }
+    }
+  }
+  // the lanes of a warp hold different columns: combine per warp, then across warps
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c) {
+    double rv = rmax[c], bv = bmax[c], xv = xmax[c];
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+      const double o = __shfl_xor_sync(0xffffffffu, rv, off);
+      rv = (o > rv || o != o) ? o : rv;
+      bv = fmax(bv, __shfl_xor_sync(0xffffffffu, bv, off));
+      xv = fmax(xv, __shfl_xor_sync(0xffffffffu, xv, off));
+    }
+    rmax[c] = rv, bmax[c] = bv, xmax[c] = xv;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) {
+      sm.red[warp][c] = rmax[c];
+      sm.red[warp][KMAX + c] = bmax[c];
+      sm.red[warp][2 * KMAX + c] = xmax[c];
+    }
+    sm.red[warp][3 * KMAX] = amax;
+  }
+  __syncthreads();
+  double berr = 0.0;
+  bool nan = false;
+  if (first) {
+    double an = 0.0;
+    for (int w = 0; w < WARPS; ++w) an = fmax(an, sm.red[w][3 * KMAX]);
+    if (tid == 0) sm.anorm = an;
+    for (int c = 0; c < k; ++c) {
+      double bn = 0.0;
+      for (int w = 0; w < WARPS; ++w) bn = fmax(bn, sm.red[w][KMAX + c]);
+      if (tid == 0) sm.bnorm[c] = bn;
+    }
+  }
+  __syncthreads();
+  for (int c = 0; c < k; ++c) {
+    double rn = 0.0, xn = 0.0;
+    for (int w = 0; w < WARPS; ++w) {
+      const double o = sm.red[w][c];
+      rn = (o > rn || o != o) ? o : rn;
+      xn = fmax(xn, sm.red[w][2 * KMAX + c]);
+    }
+    nan |= rn != rn;
+    const double den = sm.anorm * xn + sm.bnorm[c];
+    berr = fmax(berr, den > 0.0 ? rn / den : rn);
+  }
+  __syncthreads();
+  return nan ? __longlong_as_double(0x7ff8000000000000ll) : berr;
+}
+
+struct Batch {
+  int first, last;  // items [first, last) of the processing order
+  const int* sys;   // item -> system
+  const int* nb;    // item -> panel width (16 or 32)
+  const int* n;
+  const int* k;
+  const int64_t* a_off;
+  const int64_t* b_off;
+  const int64_t* x_off;
+  const int64_t* w_off;  // bytes
+  const double* a;
+  const double* b;
+  double* x;
+  unsigned char* w;
+  int method;  // RM_METHOD_*
+  int max_it;
+  double tol;  // 0: n * 2^-53
+  int fallback;
+  double* berr;  // per system
+  int* iters;
+  int* flags;
+  int* counter;
+};
+
+template <typename T, int NB>
+__device__ bool factor_and_solve(Batch& bt, Smem& sm, int n, int k, int ld, T* W, const double* a, const double* b,
+                                 int& my_pos) {
+  load_w<T>(a, n, W, ld);
+  if (threadIdx.x == 0) sm.zero_pivot = 0;
+  __syncthreads();
+  bfactor<T, NB>(W, ld, n, sm, my_pos);
+  T v[KMAX];
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)b[(int64_t)threadIdx.x * k + c] : T(0);
+  bsolve<T, NB>(W, ld, n, k, sm, my_pos, v);
+  if (my_pos >= 0)
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) sm.xs[my_pos][c] = (double)v[c];
+  __syncthreads();
+  return sm.zero_pivot == 0;
+}
+
+template <typename T, int NB>
+__device__ void correct(Batch& bt, Smem& sm, int n, int k, int ld, const T* W, int my_pos) {
+  T v[KMAX];
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)sm.rs[threadIdx.x][c] : T(0);
+  bsolve<T, NB>(W, ld, n, k, sm, my_pos, v);
+  if (my_pos >= 0)
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) sm.xs[my_pos][c] += (double)v[c];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(THREADS, 2) batch_solve_kernel(Batch bt) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  Smem& sm = *reinterpret_cast<Smem*>(dsm);
+  __shared__ int item_s;
+  for (;;) {
+    if (threadIdx.x == 0) item_s = bt.first + atomicAdd(bt.counter, 1);
+    __syncthreads();
+    const int item = item_s;
+    __syncthreads();
+    if (item >= bt.last) return;
+    const int s = bt.sys[item], nb = bt.nb[item];
+    const int n = bt.n[s], k = bt.k[s];
+    const int ld = (n + 3) & ~3;
+    const double* a = bt.a + bt.a_off[s];
+    const double* b = bt.b + bt.b_off[s];
+    double* x = bt.x + bt.x_off[s];
+    unsigned char* w = bt.w + bt.w_off[s];
+    if (threadIdx.x == 0) sm.anorm = -1.0;
+    int my_pos = -1, iters = 0, flags = 0;
+    double berr = 0.0;
+    bool done = false;
+    if (bt.method == RM_METHOD_F32_IR) {
+      float* W = reinterpret_cast<float*>(w);
+      if (nb == 32) factor_and_solve<float, 32>(bt, sm, n, k, ld, W, a, b, my_pos);
+      else factor_and_solve<float, 16>(bt, sm, n, k, ld, W, a, b, my_pos);
+      const double tol = bt.tol > 0.0 ? bt.tol : (double)n * 0x1.0p-53;
+      double prev = INFINITY;
+      for (;;) {
+        berr = bresidual(a, b, n, k, sm);
+        if (berr <= tol) {
+          done = true;
+          break;
+        }
+        if (!(berr < 0.5 * prev) || iters == bt.max_it) break;
+        prev = berr;
+        if (nb == 32) correct<float, 32>(bt, sm, n, k, ld, W, my_pos);
+        else correct<float, 16>(bt, sm, n, k, ld, W, my_pos);
+        ++iters;
+      }
+      if (!done) flags |= bt.fallback ? FLAG_FELL_BACK : FLAG_NO_CONVERGENCE;
+    }
+    if (!done && (bt.method != RM_METHOD_F32_IR || bt.fallback)) {
+      double* W = reinterpret_cast<double*>(w);
+      const bool nonzero = factor_and_solve<double, 16>(bt, sm, n, k, ld, W, a, b, my_pos);
+      berr = bresidual(a, b, n, k, sm);
+      // rustymath's `regular`: every |u_ii| > eps * n * max|a| (a NaN pivot counts as regular)
+      __shared__ int irregular;
+      if (threadIdx.x == 0) irregular = nonzero ? 0 : 1;
+      __syncthreads();
+      double amax = 0.0;
+      for (int e = threadIdx.x; e < n * n; e += THREADS) amax = fmax(amax, fabs(a[e]));
+#pragma unroll
+      for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+      if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5][0] = amax;
+      __syncthreads();
+      double big = 0.0;
+      for (int q = 0; q < WARPS; ++q) big = fmax(big, sm.red[q][0]);
+      if (my_pos >= 0) {
+        const double u = W[(int64_t)threadIdx.x * ld + my_pos];
+        if (fabs(u) <= DBL_EPSILON * n * big) atomicOr(&irregular, 1);
+      }
+      __syncthreads();
+      if (irregular) flags |= FLAG_NOT_REGULAR;
+      __syncthreads();
+    }
+    // x (row-major n x k) from xs, by unknown
+    for (int e = threadIdx.x; e < n * k; e += THREADS) x[e] = sm.xs[e / k][e % k];
+    if (threadIdx.x == 0) {
+      bt.berr[s] = berr;
+      bt.iters[s] = iters;
+      bt.flags[s] = flags;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace bt
+
+// ------------------------------------------------------------------ the plan (host)
+struct BatchPlan {
+  int64_t count = 0;
+  std::vector<int> n, k, order, nb_item;
+  std::vector<int64_t> a_off, b_off, x_off, w_off;
+  rm_solve_options opts{};
+  int nb_bucket[5] = {16, 16, 32, 32, 32};  // panel width per size bucket (tuned)
+  // device
+  int *d_sys = nullptr, *d_nb = nullptr, *d_n = nullptr, *d_k = nullptr, *d_iters = nullptr, *d_flags = nullptr,
+      *d_counter = nullptr;
+  int64_t *d_aoff = nullptr, *d_boff = nullptr, *d_xoff = nullptr, *d_woff = nullptr;
+  double* d_berr = nullptr;
+  unsigned char* d_w = nullptr;
+  size_t w_bytes = 0;
+  int grid = 0;
+  cudaStream_t stream = nullptr;  // the plan's own stream, for graph capture
+  cudaGraphExec_t graph = nullptr;
+  const void* g_a = nullptr;
+  const void* g_b = nullptr;
+  const void* g_x = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+};
+
+static int bucket_of(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : n <= 192 ? 3 : 4; }
+
+static void free_plan(BatchPlan* p) {
+  if (!p) return;
+  if (p->graph) cudaGraphExecDestroy(p->graph);
+  for (void* q : {(void*)p->d_sys, (void*)p->d_nb, (void*)p->d_n, (void*)p->d_k, (void*)p->d_iters,
+                  (void*)p->d_flags, (void*)p->d_counter, (void*)p->d_aoff, (void*)p->d_boff, (void*)p->d_xoff,
+                  (void*)p->d_woff, (void*)p->d_berr, (void*)p->d_w})
+    if (q) cudaFree(q);
+  if (p->ev_in) cudaEventDestroy(p->ev_in);
+  if (p->ev_out) cudaEventDestroy(p->ev_out);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+}
+
+template <typename V>
+static int upload(V** dst, const std::vector<V>& src) {
+  RM_CUDA_TRY(cudaMalloc(dst, std::max<size_t>(src.size(), 1) * sizeof(V)));
+  if (!src.empty()) RM_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return RM_OK;
+}
+
+static int plan_build(BatchPlan* p) {
+  const int64_t cnt = p->count;
+  p->order.resize(cnt);
+  std::iota(p->order.begin(), p->order.end(), 0);
+  // largest first: the long systems start early and the short ones fill in at the end
+  std::stable_sort(p->order.begin(), p->order.end(), [&](int x, int y) { return p->n[x] > p->n[y]; });
+  p->w_off.assign(cnt, 0);
+  size_t off = 0;
+  for (int64_t i = 0; i < cnt; ++i) {
+    const int n = p->n[i];
+    p->w_off[i] = (int64_t)off;
+    off += ((size_t)n * ((n + 3) & ~3) * 8 + 255) / 256 * 256;
+  }
+  p->w_bytes = std::max<size_t>(off, 256);
+  p->nb_item.resize(cnt);
+  for (int64_t i = 0; i < cnt; ++i) p->nb_item[i] = p->nb_bucket[bucket_of(p->n[p->order[i]])];
+  RM_TRY(upload(&p->d_sys, p->order));
+  RM_TRY(upload(&p->d_nb, p->nb_item));
+  RM_TRY(upload(&p->d_n, p->n));
+  RM_TRY(upload(&p->d_k, p->k));
+  RM_TRY(upload(&p->d_aoff, p->a_off));
+  RM_TRY(upload(&p->d_boff, p->b_off));
+  RM_TRY(upload(&p->d_xoff, p->x_off));
+  RM_TRY(upload(&p->d_woff, p->w_off));
+  RM_CUDA_TRY(cudaMalloc(&p->d_berr, std::max<int64_t>(cnt, 1) * sizeof(double)));
+  RM_CUDA_TRY(cudaMalloc(&p->d_iters, std::max<int64_t>(cnt, 1) * sizeof(int)));
+  RM_CUDA_TRY(cudaMalloc(&p->d_flags, std::max<int64_t>(cnt, 1) * sizeof(int)));
+  RM_CUDA_TRY(cudaMalloc(&p->d_counter, sizeof(int)));
+  RM_CUDA_TRY(cudaMalloc(&p->d_w, p->w_bytes));
+  static bool set = false;
+  if (!set) {
+    RM_CUDA_TRY(cudaFuncSetAttribute(bt::batch_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(bt::Smem)));
+    set = true;
+  }
+  int per_sm = 0;
+  RM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bt::batch_solve_kernel, bt::THREADS,
+                                                            sizeof(bt::Smem)));
+  p->grid = std::max(1, per_sm) * device_sm_count();
+  RM_CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  RM_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
+  RM_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+  return RM_OK;
+}
+
+static bt::Batch batch_args(BatchPlan* p, const double* a, const double* b, double* x, int first, int last) {
+  bt::Batch q;
+  q.first = first, q.last = last;
+  q.sys = p->d_sys, q.nb = p->d_nb, q.n = p->d_n, q.k = p->d_k;
+  q.a_off = p->d_aoff, q.b_off = p->d_boff, q.x_off = p->d_xoff, q.w_off = p->d_woff;
+  q.a = a, q.b = b, q.x = x, q.w = p->d_w;
+  q.method = p->opts.method;
+  q.max_it = p->opts.max_iterations > 0 ? p->opts.max_iterations : 30;
+  q.tol = p->opts.tolerance;
+  q.fallback = p->opts.fallback;
+  q.berr = p->d_berr, q.iters = p->d_iters, q.flags = p->d_flags, q.counter = p->d_counter;
+  return q;
+}
+
+// the counter reset and the one persistent launch, over items [first, last)
+static int launch_batch(BatchPlan* p, const double* a, const double* b, double* x, int first, int last,
+                        cudaStream_t s) {
+  RM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, sizeof(int), s));
+  const int items = last - first;
+  const int grid = std::min(p->grid, std::max(items, 1));
+  bt::batch_solve_kernel<<<grid, bt::THREADS, sizeof(bt::Smem), s>>>(batch_args(p, a, b, x, first, last));
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
+int batch_plan_create(int64_t count, const int64_t* n, const int64_t* k, const int64_t* a_off, const int64_t* b_off,
+                      const int64_t* x_off, const rm_solve_options* opts, BatchPlan** out) {
+  if (!out || count < 0 || count > INT_MAX || (count > 0 && (!n || !k || !a_off || !b_off || !x_off)))
+    return RM_BAD_ARG;
+  for (int64_t i = 0; i < count; ++i)
+    if (n[i] < 0 || n[i] > bt::NMAX || k[i] < 0 || k[i] > bt::KMAX || a_off[i] < 0 || b_off[i] < 0 || x_off[i] < 0) {
+      set_last_message("batched systems take 0 <= n <= 256 and 0 <= k <= 8");
+      return RM_BAD_ARG;
+    }
+  BatchPlan* p = new BatchPlan();
+  p->count = count;
+  p->n.assign(n, n + count);
+  p->k.assign(k, k + count);
+  p->a_off.assign(a_off, a_off + count);
+  p->b_off.assign(b_off, b_off + count);
+  p->x_off.assign(x_off, x_off + count);
+  if (opts) p->opts = *opts;
+  else p->opts.method = RM_METHOD_F32_IR, p->opts.fallback = 1;
+  const int st = plan_build(p);
+  if (st != RM_OK) {
+    free_plan(p);
+    return st;
+  }
+  *out = p;
+  return RM_OK;
+}
+
+void batch_plan_destroy(BatchPlan* p) { free_plan(p); }
+
+// One persistent launch over every system, replayed from a CUDA graph captured on the plan's
+// own stream (re-captured when the data pointers change); ordered after prior work on s and
+// before later work on s.
+int batch_plan_execute(BatchPlan* p, const double* a, const double* b, double* x, cudaStream_t s) {
+  if (!p) return RM_BAD_ARG;
+  if (p->count == 0) return RM_OK;
+  if (!p->graph || p->g_a != a || p->g_b != b || p->g_x != x) {
+    if (p->graph) {
+      cudaGraphExecDestroy(p->graph);
+      p->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    RM_CUDA_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = launch_batch(p, a, b, x, 0, (int)p->count, p->stream);
+    const cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+    if (st != RM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    RM_CUDA_TRY(e);
+    const cudaError_t ie = cudaGraphInstantiate(&p->graph, g, 0);
+    cudaGraphDestroy(g);
+    RM_CUDA_TRY(ie);
+    p->g_a = a, p->g_b = b, p->g_x = x;
+  }
+  RM_CUDA_TRY(cudaEventRecord(p->ev_in, s));
+  RM_CUDA_TRY(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+  RM_CUDA_TRY(cudaGraphLaunch(p->graph, p->stream));
+  note_launch();  // the graph's kernel
+  RM_CUDA_TRY(cudaEventRecord(p->ev_out, p->stream));
+  RM_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_out, 0));
+  return RM_OK;
+}
+
+// Picks the panel width of each size bucket: each candidate (16, 32) runs the bucket's own
+// systems (a contiguous range of the size-sorted order) twice, timed by CUDA events; the
+// faster stays. The results are the solves of those systems (x is written).
+int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, cudaStream_t s) {
+  if (!p) return RM_BAD_ARG;
+  const int cnt = (int)p->count;
+  cudaEvent_t e0, e1;
+  RM_CUDA_TRY(cudaEventCreate(&e0));
+  RM_CUDA_TRY(cudaEventCreate(&e1));
+  int status = RM_OK;
+  for (int bk = 0; bk < 5 && status == RM_OK; ++bk) {
+    int first = cnt, last = 0;
+    for (int i = 0; i < cnt; ++i)
+      if (bucket_of(p->n[p->order[i]]) == bk) first = std::min(first, i), last = std::max(last, i + 1);
+    if (first >= last) continue;
+    float best = INFINITY;
+    int best_nb = p->nb_bucket[bk];
+    for (int cand : {16, 32}) {
+      for (int i = first; i < last; ++i) p->nb_item[i] = cand;
+      if (cudaMemcpyAsync(p->d_nb + first, p->nb_item.data() + first, (last - first) * sizeof(int),
+                          cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        status = RM_CUDA_ERROR;
+        break;
+      }
+      float t = 0.0f;
+      for (int rep = 0; rep < 2 && status == RM_OK; ++rep) {
+        cudaEventRecord(e0, s);
+        status = launch_batch(p, a, b, x, first, last, s);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) status = RM_CUDA_ERROR;
+        cudaEventElapsedTime(&t, e0, e1);
+      }
+      if (t < best) best = t, best_nb = cand;
+    }
+    p->nb_bucket[bk] = best_nb;
+    for (int i = first; i < last; ++i) p->nb_item[i] = best_nb;
+    if (cudaMemcpyAsync(p->d_nb + first, p->nb_item.data() + first, (last - first) * sizeof(int),
+                        cudaMemcpyHostToDevice, s) != cudaSuccess)
+      status = RM_CUDA_ERROR;
+  }
+  cudaStreamSynchronize(s);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return status;  // the kernel reads the widths from d_nb, so a captured graph stays valid
+}
+
+int batch_plan_results(BatchPlan* p, double* berr, int32_t* iters, int32_t* flags, rm_batch_report* summary) {
+  if (!p) return RM_BAD_ARG;
+  const int64_t cnt = p->count;
+  std::vector<double> be(cnt);
+  std::vector<int> it(cnt), fl(cnt);
+  RM_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (cnt) {
+    RM_CUDA_TRY(cudaMemcpy(be.data(), p->d_berr, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    RM_CUDA_TRY(cudaMemcpy(it.data(), p->d_iters, cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    RM_CUDA_TRY(cudaMemcpy(fl.data(), p->d_flags, cnt * sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  if (berr) std::copy(be.begin(), be.end(), berr);
+  if (iters) std::copy(it.begin(), it.end(), iters);
+  if (flags) std::copy(fl.begin(), fl.end(), flags);
+  if (summary) {
+    summary->max_backward_error = 0.0;
+    summary->fell_back = summary->not_regular = summary->no_convergence = 0;
+    summary->max_iterations = 0;
+    for (int64_t i = 0; i < cnt; ++i) {
+      summary->max_backward_error = std::max(summary->max_backward_error, be[i]);
+      if (be[i] != be[i]) summary->max_backward_error = be[i];
+      summary->fell_back += (fl[i] & bt::FLAG_FELL_BACK) != 0;
+      summary->not_regular += (fl[i] & bt::FLAG_NOT_REGULAR) != 0;
+      summary->no_convergence += (fl[i] & bt::FLAG_NO_CONVERGENCE) != 0;
+      summary->max_iterations = std::max(summary->max_iterations, it[i]);
+    }
+  }
+  return RM_OK;
+}
+
+}  // namespace rm
+
+// ------------------------------------------------------------------ C ABI
+struct rm_batch_plan {
+  rm::BatchPlan* p;
+};
+
+extern "C" {
+
+int rm_batch_plan_create(int64_t count, const int64_t* h_n, const int64_t* h_k, const int64_t* h_a_off,
+                         const int64_t* h_b_off, const int64_t* h_x_off, const rm_solve_options* opts,
+                         rm_batch_plan** plan) {
+  if (!plan) return RM_BAD_ARG;
+  *plan = nullptr;
+  RM_TRY(rm::check_device());
+  rm::BatchPlan* p = nullptr;
+  RM_TRY(rm::batch_plan_create(count, h_n, h_k, h_a_off, h_b_off, h_x_off, opts, &p));
+  *plan = new rm_batch_plan{p};
+  return RM_OK;
+}
+
+int rm_batch_plan_tune(rm_batch_plan* plan, const double* d_a, const double* d_b, double* d_x, void* stream) {
+  if (!plan || !d_a || !d_b || !d_x) return RM_BAD_ARG;
+  RM_TRY(rm::batch_plan_tune(plan->p, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream)));
+  return rm::take_device_status(reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rm_batch_plan_execute(rm_batch_plan* plan, const double* d_a, const double* d_b, double* d_x, void* stream) {
+  if (!plan || (plan->p->count > 0 && (!d_a || !d_b || !d_x))) return RM_BAD_ARG;
+  return rm::batch_plan_execute(plan->p, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rm_batch_plan_results(rm_batch_plan* plan, double* h_berr, int32_t* h_iters, int32_t* h_flags,
+                          rm_batch_report* summary) {
+  if (!plan) return RM_BAD_ARG;
+  return rm::batch_plan_results(plan->p, h_berr, h_iters, h_flags, summary);
+}
+
+int rm_batch_plan_panel_width(const rm_batch_plan* plan, int bucket) {
+  return plan && bucket >= 0 && bucket < 5 ? plan->p->nb_bucket[bucket] : 0;
+}
+
+int rm_batch_plan_destroy(rm_batch_plan* plan) {
+  if (!plan) return RM_OK;
+  rm::batch_plan_destroy(plan->p);
+  delete plan;
+  return RM_OK;
+}
+
+int rm_dsolve_batched(int64_t count, const int64_t* h_n, const int64_t* h_k, const int64_t* h_a_off,
+                      const int64_t* h_b_off, const int64_t* h_x_off, const double* d_a, const double* d_b,
+                      double* d_x, const rm_solve_options* opts, rm_batch_report* report, void* stream) {
+  rm_batch_plan* plan = nullptr;
+  RM_TRY(rm_batch_plan_create(count, h_n, h_k, h_a_off, h_b_off, h_x_off, opts, &plan));
+  int st = rm_batch_plan_execute(plan, d_a, d_b, d_x, stream);
+  if (st == RM_OK) st = rm::take_device_status(reinterpret_cast<cudaStream_t>(stream));
+  if (st == RM_OK) st = rm_batch_plan_results(plan, nullptr, nullptr, nullptr, report);
+  rm_batch_plan_destroy(plan);
+  if (st == RM_OK && report && report->no_convergence > 0) {
+    rm::set_last_message("refinement stalled on some systems and fallback was off");
+    return RM_NO_CONVERGENCE;
+  }
+  return st;
+}
+
+}  // extern "C"

@@ -100,6 +100,7 @@ unsigned* device_status();
 // Reads and clears the current device's status word (synchronises `stream`); maps bits to
 // an rm status code.
 int take_device_status(cudaStream_t stream);
+int check_device();  // RM_NO_DEVICE without a compute capability 10.x GPU
 
 // ---------------------------------------------------------------- mixed precision (mixed.cu)
 size_t getrf_lpp_f32_scratch_bytes(int64_t n);

@@ -1,0 +1,161 @@
+"""Batched solves of uneven systems (rm_dsolve_batched / rm_batch_plan_*), checked system by
+system against the oracle: the normwise backward error (double-double residual) must be at
+most n * 2^-53 for the mixed method, and the plain float64 method must agree with the
+oracle's solve within the forward error kappa * n * eps allows."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+EPS = np.finfo(np.float64).eps
+EDGE = [1, 2, 3, 8, 15, 16, 17, 31, 32, 33, 63, 64, 65, 127, 128, 129, 191, 192, 193, 255, 256]
+
+
+@pytest.fixture(scope="module")
+def rb():
+    import rustymath_b200 as rb
+    return rb
+
+
+def shifted(n, k, seed):
+    """The batched configuration's systems: A = N(0,1) + n I, B = N(0,1)."""
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((n, n)) + n * np.eye(n), rng.standard_normal((n, k))
+
+
+def general(n, k, seed):
+    """N(0,1) matrices: row exchanges matter."""
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((n, n)), rng.standard_normal((n, k))
+
+
+def batch(sizes, ks, make, seed=0):
+    As, Bs = [], []
+    for i, (n, k) in enumerate(zip(sizes, ks)):
+        a, b = make(n, k, seed + i)
+        As.append(a)
+        Bs.append(b)
+    return As, Bs
+
+
+def check_bar(As, Bs, Xs):
+    for a, b, x in zip(As, Bs, Xs):
+        n = a.shape[0]
+        assert O.backward_error(a, x, b) <= max(n, 1) * 2.0 ** -53, n
+
+
+def test_mixed_uneven_edges(rb):
+    rng = np.random.default_rng(1)
+    sizes = EDGE + list(rng.integers(8, 257, 60))
+    ks = list(rng.integers(1, 9, len(sizes)))
+    As, Bs = batch(sizes, ks, shifted)
+    Xs, rep = rb.solve_batched(As, Bs, method="mixed")
+    check_bar(As, Bs, Xs)
+    assert rep.fell_back == 0 and rep.not_regular == 0
+    assert rep.max_backward_error <= 256 * 2.0 ** -53
+    assert 1 <= rep.max_iterations <= 3
+
+
+def test_mixed_general_matrices_need_pivots(rb):
+    rng = np.random.default_rng(2)
+    sizes = [5, 33, 100, 200, 256, 129, 64]
+    As, Bs = batch(sizes, [3] * len(sizes), general, seed=10)
+    Xs, rep = rb.solve_batched(As, Bs, method="mixed")
+    check_bar(As, Bs, Xs)
+    for a, b, x in zip(As, Bs, Xs):
+        xo = O.solve(a, b)
+        kappa = np.linalg.cond(a)
+        assert np.abs(x - xo).max() <= kappa * a.shape[0] * EPS * np.abs(xo).max()
+
+
+def test_plain_matches_oracle(rb):
+    sizes = [1, 7, 32, 90, 256, 150]
+    As, Bs = batch(sizes, [2, 1, 8, 4, 3, 5], general, seed=20)
+    Xs, rep = rb.solve_batched(As, Bs, method="plain")
+    assert rep.fell_back == 0 and rep.max_iterations == 0
+    for a, b, x in zip(As, Bs, Xs):
+        xo = O.solve(a, b)
+        kappa = np.linalg.cond(a)
+        assert np.abs(x - xo).max() <= kappa * a.shape[0] * EPS * np.abs(xo).max()
+    check_bar(As, Bs, Xs)
+
+
+def test_stall_falls_back_and_singular_is_flagged(rb):
+    from rustymath_b200 import _lib
+    n = 120
+    rng = np.random.default_rng(3)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    hard = (u * np.logspace(0, -12, n)) @ v.T  # beyond float32 factors' reach
+    As = [shifted(40, 2, 4)[0], hard, np.ones((9, 9)), shifted(200, 1, 5)[0]]
+    Bs = [rng.standard_normal((40, 2)), rng.standard_normal((n, 3)), np.ones((9, 1)), rng.standard_normal((200, 1))]
+    plan = rb.BatchPlan([a.shape[0] for a in As], [b.shape[1] for b in Bs], method="mixed")
+    a, b = plan.pack(As, Bs, device="cuda")
+    import torch
+    x = torch.zeros(plan.b_size, dtype=torch.float64, device="cuda")
+    plan.execute(a, b, x)
+    berr, iters, flags, rep = plan.results()
+    Xs = [t.cpu().numpy() for t in plan.unpack(x)]
+    assert flags[0] == 0 and flags[3] == 0
+    assert flags[1] & _lib.RM_BATCH_FELL_BACK and not flags[1] & _lib.RM_BATCH_NOT_REGULAR
+    assert flags[2] & _lib.RM_BATCH_NOT_REGULAR
+    assert rep.fell_back == 2 and rep.not_regular == 1
+    for i in (0, 1, 3):
+        assert O.backward_error(As[i], Xs[i], Bs[i]) <= As[i].shape[0] * 2.0 ** -53
+    plan.close()
+
+
+def test_empty_systems_and_empty_batch(rb):
+    As = [np.zeros((0, 0)), shifted(10, 1, 6)[0], np.zeros((0, 0))]
+    Bs = [np.zeros((0, 1)), np.ones((10, 1)), np.zeros((0, 2))]
+    Xs, rep = rb.solve_batched(As, Bs)
+    assert Xs[0].shape == (0, 1) and Xs[2].shape == (0, 2)
+    check_bar(As[1:2], Bs[1:2], Xs[1:2])
+    Xs, rep = rb.solve_batched([], [])
+    assert Xs == []
+
+
+def test_too_large_is_rejected(rb):
+    with pytest.raises(ValueError):
+        rb.BatchPlan([257], [1])
+    with pytest.raises(ValueError):
+        rb.BatchPlan([10], [9])
+
+
+def test_tune_and_graph_replay(rb):
+    import torch
+    rng = np.random.default_rng(7)
+    sizes = list(rng.integers(8, 257, 300))
+    ks = list(rng.integers(1, 5, 300))
+    As, Bs = batch(sizes, ks, shifted, seed=100)
+    plan = rb.BatchPlan(sizes, ks, method="mixed")
+    a, b = plan.pack(As, Bs, device="cuda")
+    x = torch.zeros(plan.b_size, dtype=torch.float64, device="cuda")
+    widths = plan.tune(a, b, x)
+    assert all(w in (16, 32) for w in widths)
+    plan.execute(a, b, x)
+    check_bar(As, Bs, [t.cpu().numpy() for t in plan.unpack(x)])
+    # the same pointers replay the captured graph; new right-hand sides in place
+    Bs2 = [rng.standard_normal(bb.shape) for bb in Bs]
+    _, b2 = plan.pack(As, Bs2, device="cuda")
+    b.copy_(b2)
+    plan.execute(a, b, x)
+    torch.cuda.synchronize()
+    check_bar(As, Bs2, [t.cpu().numpy() for t in plan.unpack(x)])
+    # new pointers capture again
+    x2 = torch.zeros_like(x)
+    plan.execute(a, b, x2)
+    torch.cuda.synchronize()
+    assert torch.equal(x, x2)
+    plan.close()
+
+
+def test_device_lists(rb):
+    import torch
+    As, Bs = batch([50, 130], [2, 1], shifted, seed=30)
+    ta = [torch.tensor(a, device="cuda") for a in As]
+    tb = [torch.tensor(b[:, 0], device="cuda") if b.shape[1] == 1 else torch.tensor(b, device="cuda") for b in Bs]
+    Xs, rep = rb.solve_batched(ta, tb)
+    assert Xs[1].shape == (130,) and Xs[1].is_cuda
+    check_bar(As, Bs, [Xs[0].cpu().numpy(), Xs[1].cpu().numpy().reshape(-1, 1)])
