@@ -171,6 +171,18 @@ int rm_batch_plan_execute(rm_batch_plan *plan, const double *d_a, const double *
  * pointer may be NULL); synchronises. */
 int rm_batch_plan_results(rm_batch_plan *plan, double *h_berr, int32_t *h_iters, int32_t *h_flags,
                           rm_batch_report *summary);
+/* The adjoint of the last execute, for reverse-mode differentiation of x = A^-1 b: given
+ * d_gx = dL/dx (packed like b), writes d_gb = dL/db = A^-T dL/dx (packed like b) and, unless
+ * d_ga is NULL, d_ga = dL/dA = -(dL/db) x^T (packed like a). It reuses the factors the
+ * execute left in the plan (d_a and d_x must be that execute's): a transposed solve with the
+ * same row order, refined in float64 against A^T when the factors are float32 (an A whose
+ * refinement stalls is factored again in float64). rustymath has no derivative of solve; this
+ * is the north star's adjoint. Asynchronous on `stream`. */
+int rm_batch_plan_adjoint(rm_batch_plan *plan, const double *d_a, const double *d_x, const double *d_gx,
+                          double *d_gb, double *d_ga, void *stream);
+/* Per-system normwise backward errors of the last adjoint's A^T gb = gx (either pointer may be
+ * NULL); synchronises. */
+int rm_batch_plan_adjoint_results(rm_batch_plan *plan, double *h_berr, double *h_max_berr);
 /* The panel width chosen for size bucket 0..4 (n <= 32, 64, 128, 192, 256). */
 int rm_batch_plan_panel_width(const rm_batch_plan *plan, int bucket);
 int rm_batch_plan_destroy(rm_batch_plan *plan);

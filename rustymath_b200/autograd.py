@@ -1,0 +1,58 @@
+"""Reverse-mode differentiation of batched solves: `solve(a, b)` for stacks of systems as a
+torch.autograd.Function.
+
+The forward pass is the batched solve (one persistent launch, rustymath_b200.batched); the
+backward pass is the hand-written adjoint kernel: for x = A^-1 b and an upstream gradient
+g = dL/dx, dL/db = A^-T g (a transposed solve reusing the forward's LU factors and row
+order, refined in float64 against A^T) and dL/dA = -(dL/db) x^T (the rank-k outer product,
+formed in the same kernel). rustymath's solve has no derivative; the shapes follow its stack
+convention (the matrices in the last two axes).
+"""
+import torch
+
+from .batched import BatchPlan
+
+__all__ = ["solve", "BatchedSolve"]
+
+
+class BatchedSolve(torch.autograd.Function):
+    """x = A^-1 b for a (batch, n, n) float64 CUDA stack and (batch, n, k) right-hand sides."""
+
+    @staticmethod
+    def forward(ctx, a, b, method):
+        batch, n, _ = a.shape
+        k = b.shape[-1]
+        plan = BatchPlan([n] * batch, [k] * batch, method=method)
+        af = a.detach().contiguous().view(-1)
+        bf = b.detach().contiguous().view(-1)
+        x = torch.empty(batch * n * k, dtype=torch.float64, device=a.device)
+        if batch:
+            plan.execute(af, bf, x)
+        ctx.plan = plan
+        ctx.shapes = (batch, n, k)
+        ctx.save_for_backward(af, x)
+        return x.view(batch, n, k)
+
+    @staticmethod
+    def backward(ctx, gx):
+        af, x = ctx.saved_tensors
+        batch, n, k = ctx.shapes
+        plan = ctx.plan
+        gb = torch.empty(batch * n * k, dtype=torch.float64, device=x.device)
+        ga = torch.empty(batch * n * n, dtype=torch.float64, device=x.device) if ctx.needs_input_grad[0] else None
+        if batch:
+            plan.adjoint(af, x, gx.detach().to(torch.float64).contiguous().view(-1), gb, ga)
+        return (None if ga is None else ga.view(batch, n, n)), gb.view(batch, n, k), None
+
+
+def solve(a, b, method="mixed"):
+    """x with a[i] x[i] = b[i] for a stack a (batch, n, n) and b (batch, n, k) or (batch, n),
+    float64 CUDA tensors, n <= 256 and k <= 8; differentiable in a and b."""
+    if a.ndim != 3 or a.shape[-1] != a.shape[-2]:
+        raise ValueError("solve needs a (batch, n, n) stack")
+    vector = b.ndim == 2
+    bb = b.unsqueeze(-1) if vector else b
+    if bb.shape[:2] != a.shape[:2]:
+        raise ValueError("b's leading axes must match a's stack and rows")
+    x = BatchedSolve.apply(a.to(torch.float64), bb.to(torch.float64), method)
+    return x.squeeze(-1) if vector else x

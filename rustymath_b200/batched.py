@@ -88,6 +88,29 @@ class BatchPlan:
         """One persistent launch for every system (asynchronous on the current stream)."""
         check(_lib.load().rm_batch_plan_execute(self._h, *self._ptrs(a, b, x)), "batch execute")
 
+    def adjoint(self, a, x, gx, gb, ga=None):
+        """gb = A^-T gx and (unless ga is None) ga = -gb x^T for every system, from the factors
+        of the last execute (a and x must be that execute's); asynchronous."""
+        torch = _torch()
+        for t in (gx, gb) + (() if ga is None else (ga,)):
+            if not (_is_torch(t) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("BatchPlan works on contiguous float64 CUDA tensors")
+        if gx.numel() < self.b_size or gb.numel() < self.b_size or (ga is not None and ga.numel() < self.a_size):
+            raise ValueError("the packed arrays are smaller than the plan's shapes")
+        pa, _, px, ps = self._ptrs(a, gx, x)
+        check(_lib.load().rm_batch_plan_adjoint(self._h, pa, px, ctypes.c_void_p(gx.data_ptr()),
+                                                ctypes.c_void_p(gb.data_ptr()),
+                                                None if ga is None else ctypes.c_void_p(ga.data_ptr()), ps),
+              "batch adjoint")
+
+    def adjoint_results(self):
+        """(per-system backward errors of A^T gb = gx, their maximum) of the last adjoint."""
+        berr = np.zeros(self.count)
+        mx = ctypes.c_double()
+        check(_lib.load().rm_batch_plan_adjoint_results(self._h, berr.ctypes.data if self.count else None,
+                                                        ctypes.byref(mx)), "batch adjoint results")
+        return berr, mx.value
+
     def results(self):
         """(backward errors, refinement steps, RM_BATCH_* flags, BatchReport) of the last execute."""
         berr = np.zeros(self.count)

@@ -426,6 +426,9 @@ struct Batch {
   int* iters;
   int* flags;
   int* counter;
+  int* piv;            // per system (at p_off): the row chosen for each logical column
+  const int64_t* p_off;
+  int* ftype;          // per system: 0 when W holds float32 factors, 1 for float64
 };
 
 template <typename T, int NB>
@@ -523,13 +526,286 @@ __global__ void __launch_bounds__(THREADS, 2) batch_solve_kernel(Batch bt) {
       if (irregular) flags |= FLAG_NOT_REGULAR;
       __syncthreads();
     }
-    // x (row-major n x k) from xs, by unknown
+    // x (row-major n x k) from xs, by unknown; the factors' row order and type stay for the adjoint
     for (int e = threadIdx.x; e < n * k; e += THREADS) x[e] = sm.xs[e / k][e % k];
+    for (int i = threadIdx.x; i < n; i += THREADS) bt.piv[bt.p_off[s] + i] = sm.piv[i];
     if (threadIdx.x == 0) {
       bt.berr[s] = berr;
       bt.iters[s] = iters;
       bt.flags[s] = flags;
+      bt.ftype[s] = (bt.method == RM_METHOD_F32_IR && (done || !bt.fallback)) ? 0 : 1;
     }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ the adjoint
+// Solves A^T y = g with the implicitly pivoted factors of bfactor (P A = L U, row piv[i] of A
+// at logical position i): U^T z = g, then L^T w = z, then y[piv[i]] = w_i. Thread t holds
+// v = g_t (column t, the unknowns' order) on entry and w_t on return. U^T and L^T are solved
+// in blocks of NB: a warp solves the diagonal block with shuffles; then each thread updates
+// its own column from the block's rows (coalesced: consecutive threads, consecutive columns).
+template <typename T, int NB>
+__device__ void bsolve_t(const T* W, int ld, int n, int k, Smem& sm, T (&v)[KMAX]) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int J = 0; J < n; J += NB) {  // U^T z = g: lower triangle, forward
+    const int nbj = min(NB, n - J);
+    if (t >= J && t < J + nbj)
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) sm.vsm[t - J][c] = (double)v[c];
+    __syncthreads();
+    if (warp == 0) {
+      T y[KMAX], ucol[NB];
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+#pragma unroll
+      for (int q = 0; q < NB; ++q)  // U[J+q][J+lane], q <= lane
+        ucol[q] = (lane < nbj && q <= lane) ? W[(int64_t)sm.piv[J + q] * ld + J + lane] : T(0);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        if (q < nbj) {
+#pragma unroll
+          for (int c = 0; c < KMAX; ++c) {
+            if (c < k) {
+              if (lane == q) y[c] = y[c] / ucol[q];
+              const T zq = __shfl_sync(0xffffffffu, y[c], q);
+              if (lane > q) y[c] = fma(-ucol[q], zq, y[c]);
+            }
+          }
+        }
+      }
+      if (lane < nbj)
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+    }
+    __syncthreads();
+    if (t < n) {
+      if (t >= J + nbj) {
+        for (int q = 0; q < nbj; ++q) {
+          const T u = W[(int64_t)sm.piv[J + q] * ld + t];
+#pragma unroll
+          for (int c = 0; c < KMAX; ++c)
+            if (c < k) v[c] = fma(-u, (T)sm.vsm[q][c], v[c]);
+        }
+      } else if (t >= J) {
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) v[c] = (T)sm.vsm[t - J][c];
+      }
+    }
+    __syncthreads();
+  }
+  const int last = (n - 1) / NB * NB;
+  for (int J = last; J >= 0; J -= NB) {  // L^T w = z: unit upper triangle, backward
+    const int nbj = min(NB, n - J);
+    if (t >= J && t < J + nbj)
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) sm.vsm[t - J][c] = (double)v[c];
+    __syncthreads();
+    if (warp == 0) {
+      T y[KMAX], lcol[NB];
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+#pragma unroll
+      for (int q = 0; q < NB; ++q)  // L[J+q][J+lane], q > lane
+        lcol[q] = (lane < nbj && q > lane && q < nbj) ? W[(int64_t)sm.piv[J + q] * ld + J + lane] : T(0);
+#pragma unroll
+      for (int q = NB - 1; q >= 0; --q) {
+        if (q < nbj) {
+#pragma unroll
+          for (int c = 0; c < KMAX; ++c) {
+            if (c < k) {
+              const T wq = __shfl_sync(0xffffffffu, y[c], q);
+              if (lane < q) y[c] = fma(-lcol[q], wq, y[c]);
+            }
+          }
+        }
+      }
+      if (lane < nbj)
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+    }
+    __syncthreads();
+    if (t < n) {
+      if (t < J) {
+        for (int q = 0; q < nbj; ++q) {
+          const T l = W[(int64_t)sm.piv[J + q] * ld + t];
+#pragma unroll
+          for (int c = 0; c < KMAX; ++c)
+            if (c < k) v[c] = fma(-l, (T)sm.vsm[q][c], v[c]);
+        }
+      } else if (t < J + nbj) {
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) v[c] = (T)sm.vsm[t - J][c];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// sm.rs[t] = g_t - (A^T y)_t (by column t; y = sm.xs by row) for the n x n row-major a, and
+// the normwise backward error of A^T y = g (NaN if a residual is NaN).
+__device__ double bresidual_t(const double* __restrict__ a, const double* __restrict__ g, int n, int k, Smem& sm) {
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  double r[KMAX], gv[KMAX], yv[KMAX], asum = 0.0;
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c) r[c] = gv[c] = yv[c] = 0.0;
+  if (t < n) {
+    double acc[KMAX];
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) acc[c] = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double av = __ldg(a + (int64_t)i * n + t);  // column t: coalesced across threads
+      asum += fabs(av);
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c)
+        if (c < k) acc[c] = fma(av, sm.xs[i][c], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c)
+      if (c < k) {
+        gv[c] = g[(int64_t)t * k + c];
+        r[c] = gv[c] - acc[c];
+        yv[c] = fabs(sm.xs[t][c]);
+        sm.rs[t][c] = r[c];
+      }
+  }
+  double rm[KMAX], gm[KMAX], ym[KMAX];
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c) {
+    double rv = fabs(r[c]), gvv = fabs(gv[c]), yvv = yv[c];
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+      const double o = __shfl_xor_sync(0xffffffffu, rv, off);
+      rv = (o > rv || o != o) ? o : rv;
+      gvv = fmax(gvv, __shfl_xor_sync(0xffffffffu, gvv, off));
+      yvv = fmax(yvv, __shfl_xor_sync(0xffffffffu, yvv, off));
+    }
+    rm[c] = rv, gm[c] = gvv, ym[c] = yvv;
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) asum = fmax(asum, __shfl_xor_sync(0xffffffffu, asum, off));
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) {
+      sm.red[warp][c] = rm[c];
+      sm.red[warp][KMAX + c] = gm[c];
+      sm.red[warp][2 * KMAX + c] = ym[c];
+    }
+    sm.red[warp][3 * KMAX] = asum;
+  }
+  __syncthreads();
+  double an = 0.0, berr = 0.0;
+  bool nan = false;
+  for (int w = 0; w < WARPS; ++w) an = fmax(an, sm.red[w][3 * KMAX]);
+  for (int c = 0; c < k; ++c) {
+    double rn = 0.0, gn = 0.0, yn = 0.0;
+    for (int w = 0; w < WARPS; ++w) {
+      const double o = sm.red[w][c];
+      rn = (o > rn || o != o) ? o : rn;
+      gn = fmax(gn, sm.red[w][KMAX + c]);
+      yn = fmax(yn, sm.red[w][2 * KMAX + c]);
+    }
+    nan |= rn != rn;
+    const double den = an * yn + gn;
+    berr = fmax(berr, den > 0.0 ? rn / den : rn);
+  }
+  __syncthreads();
+  return nan ? __longlong_as_double(0x7ff8000000000000ll) : berr;
+}
+
+struct Adjoint {
+  Batch bt;             // the forward's layout, factors (w), row orders (piv) and types
+  const double* g;      // dL/dx, packed like b
+  double* gb;           // dL/db = A^-T g, packed like b
+  double* ga;           // dL/dA = -gb x^T, packed like a (NULL: not formed)
+  double* berr;         // per system: the backward error of A^T gb = g
+};
+
+template <typename T, int NB>
+__device__ void adjoint_solve(const Adjoint& aj, Smem& sm, int n, int k, int ld, const T* W, const double* g,
+                              bool add) {
+  T v[KMAX];
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c)
+    v[c] = (threadIdx.x < n && c < k) ? (T)(add ? sm.rs[threadIdx.x][c] : g[(int64_t)threadIdx.x * k + c]) : T(0);
+  bsolve_t<T, NB>(W, ld, n, k, sm, v);
+  if (threadIdx.x < n) {
+    const int row = sm.piv[threadIdx.x];
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c) sm.xs[row][c] = add ? sm.xs[row][c] + (double)v[c] : (double)v[c];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(THREADS, 2) batch_adjoint_kernel(Adjoint aj) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  Smem& sm = *reinterpret_cast<Smem*>(dsm);
+  __shared__ int item_s;
+  const Batch& bt = aj.bt;
+  for (;;) {
+    if (threadIdx.x == 0) item_s = bt.first + atomicAdd(bt.counter, 1);
+    __syncthreads();
+    const int item = item_s;
+    __syncthreads();
+    if (item >= bt.last) return;
+    const int s = bt.sys[item];
+    const int n = bt.n[s], k = bt.k[s];
+    const int ld = (n + 3) & ~3;
+    const double* a = bt.a + bt.a_off[s];
+    const double* g = aj.g + bt.b_off[s];
+    unsigned char* w = bt.w + bt.w_off[s];
+    for (int i = threadIdx.x; i < n; i += THREADS) sm.piv[i] = bt.piv[bt.p_off[s] + i];
+    __syncthreads();
+    double berr = 0.0;
+    const double tol = bt.tol > 0.0 ? bt.tol : (double)n * 0x1.0p-53;
+    bool done = false;
+    if (bt.ftype[s] == 0) {
+      // float32 factors: refine in float64 against A^T
+      const float* W = reinterpret_cast<const float*>(w);
+      adjoint_solve<float, 32>(aj, sm, n, k, ld, W, g, false);
+      double prev = INFINITY;
+      for (int it = 0;; ++it) {
+        berr = bresidual_t(a, g, n, k, sm);
+        if (berr <= tol) {
+          done = true;
+          break;
+        }
+        if (!(berr < 0.5 * prev) || it == bt.max_it) break;
+        prev = berr;
+        adjoint_solve<float, 32>(aj, sm, n, k, ld, W, g, true);
+      }
+    }
+    if (!done) {
+      // float64 factors (the forward's, or made here when float32 refinement stalls)
+      double* W = reinterpret_cast<double*>(w);
+      if (bt.ftype[s] == 0) {
+        load_w<double>(a, n, W, ld);
+        __syncthreads();
+        int my_pos;
+        bfactor<double, 16>(W, ld, n, sm, my_pos);
+        for (int i = threadIdx.x; i < n; i += THREADS) bt.piv[bt.p_off[s] + i] = sm.piv[i];
+        if (threadIdx.x == 0) bt.ftype[s] = 1;
+        __syncthreads();
+      }
+      adjoint_solve<double, 16>(aj, sm, n, k, ld, W, g, false);
+      berr = bresidual_t(a, g, n, k, sm);
+    }
+    // gb (packed like b) and ga = -gb x^T (packed like a)
+    double* gb = aj.gb + bt.b_off[s];
+    for (int e = threadIdx.x; e < n * k; e += THREADS) gb[e] = sm.xs[e / k][e % k];
+    if (aj.ga) {
+      const double* x = bt.x + bt.x_off[s];
+      for (int e = threadIdx.x; e < n * k; e += THREADS) sm.rs[e / k][e % k] = x[e];
+      __syncthreads();
+      double* ga = aj.ga + bt.a_off[s];
+      for (int e = threadIdx.x; e < n * n; e += THREADS) {
+        const int i = e / n, j = e - i * n;
+        double acc = 0.0;
+        for (int c = 0; c < k; ++c) acc = fma(sm.xs[i][c], sm.rs[j][c], acc);
+        ga[e] = -acc;
+      }
+    }
+    if (threadIdx.x == 0) aj.berr[s] = berr;
     __syncthreads();
   }
 }
@@ -546,8 +822,10 @@ struct BatchPlan {
   // device
   int *d_sys = nullptr, *d_nb = nullptr, *d_n = nullptr, *d_k = nullptr, *d_iters = nullptr, *d_flags = nullptr,
       *d_counter = nullptr;
-  int64_t *d_aoff = nullptr, *d_boff = nullptr, *d_xoff = nullptr, *d_woff = nullptr;
+  int64_t *d_aoff = nullptr, *d_boff = nullptr, *d_xoff = nullptr, *d_woff = nullptr, *d_poff = nullptr;
+  int *d_piv = nullptr, *d_ftype = nullptr;
   double* d_berr = nullptr;
+  double* d_adj_berr = nullptr;
   unsigned char* d_w = nullptr;
   size_t w_bytes = 0;
   int grid = 0;
@@ -566,7 +844,8 @@ static void free_plan(BatchPlan* p) {
   if (p->graph) cudaGraphExecDestroy(p->graph);
   for (void* q : {(void*)p->d_sys, (void*)p->d_nb, (void*)p->d_n, (void*)p->d_k, (void*)p->d_iters,
                   (void*)p->d_flags, (void*)p->d_counter, (void*)p->d_aoff, (void*)p->d_boff, (void*)p->d_xoff,
-                  (void*)p->d_woff, (void*)p->d_berr, (void*)p->d_w})
+                  (void*)p->d_woff, (void*)p->d_berr, (void*)p->d_w, (void*)p->d_poff, (void*)p->d_piv,
+                  (void*)p->d_ftype, (void*)p->d_adj_berr})
     if (q) cudaFree(q);
   if (p->ev_in) cudaEventDestroy(p->ev_in);
   if (p->ev_out) cudaEventDestroy(p->ev_out);
@@ -605,6 +884,13 @@ static int plan_build(BatchPlan* p) {
   RM_TRY(upload(&p->d_boff, p->b_off));
   RM_TRY(upload(&p->d_xoff, p->x_off));
   RM_TRY(upload(&p->d_woff, p->w_off));
+  std::vector<int64_t> p_off(cnt);
+  int64_t poff = 0;
+  for (int64_t i = 0; i < cnt; ++i) p_off[i] = poff, poff += p->n[i];
+  RM_TRY(upload(&p->d_poff, p_off));
+  RM_CUDA_TRY(cudaMalloc(&p->d_piv, std::max<int64_t>(poff, 1) * sizeof(int)));
+  RM_CUDA_TRY(cudaMalloc(&p->d_ftype, std::max<int64_t>(cnt, 1) * sizeof(int)));
+  RM_CUDA_TRY(cudaMalloc(&p->d_adj_berr, std::max<int64_t>(cnt, 1) * sizeof(double)));
   RM_CUDA_TRY(cudaMalloc(&p->d_berr, std::max<int64_t>(cnt, 1) * sizeof(double)));
   RM_CUDA_TRY(cudaMalloc(&p->d_iters, std::max<int64_t>(cnt, 1) * sizeof(int)));
   RM_CUDA_TRY(cudaMalloc(&p->d_flags, std::max<int64_t>(cnt, 1) * sizeof(int)));
@@ -613,6 +899,8 @@ static int plan_build(BatchPlan* p) {
   static bool set = false;
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(bt::batch_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(bt::Smem)));
+    RM_CUDA_TRY(cudaFuncSetAttribute(bt::batch_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(bt::Smem)));
     set = true;
   }
@@ -637,6 +925,7 @@ static bt::Batch batch_args(BatchPlan* p, const double* a, const double* b, doub
   q.tol = p->opts.tolerance;
   q.fallback = p->opts.fallback;
   q.berr = p->d_berr, q.iters = p->d_iters, q.flags = p->d_flags, q.counter = p->d_counter;
+  q.piv = p->d_piv, q.p_off = p->d_poff, q.ftype = p->d_ftype;
   return q;
 }
 
@@ -760,6 +1049,40 @@ int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, c
   return status;  // the kernel reads the widths from d_nb, so a captured graph stays valid
 }
 
+// dL/db = A^-T g and dL/dA = -(dL/db) x^T for every system, from the factors the last
+// execute left in the plan (the same a and x); one persistent launch on the plan's stream,
+// ordered after prior work on s and before later work on s.
+int batch_plan_adjoint(BatchPlan* p, const double* a, const double* x, const double* g, double* gb, double* ga,
+                       cudaStream_t s) {
+  if (!p) return RM_BAD_ARG;
+  if (p->count == 0) return RM_OK;
+  RM_CUDA_TRY(cudaEventRecord(p->ev_in, s));
+  RM_CUDA_TRY(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+  RM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, sizeof(int), p->stream));
+  bt::Adjoint aj;
+  aj.bt = batch_args(p, a, nullptr, const_cast<double*>(x), 0, (int)p->count);
+  aj.g = g, aj.gb = gb, aj.ga = ga, aj.berr = p->d_adj_berr;
+  const int grid = std::min<int64_t>(p->grid, p->count);
+  bt::batch_adjoint_kernel<<<grid, bt::THREADS, sizeof(bt::Smem), p->stream>>>(aj);
+  RM_LAUNCHED();
+  RM_CUDA_TRY(cudaEventRecord(p->ev_out, p->stream));
+  RM_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_out, 0));
+  return RM_OK;
+}
+
+int batch_plan_adjoint_results(BatchPlan* p, double* berr, double* max_berr) {
+  if (!p) return RM_BAD_ARG;
+  std::vector<double> be(p->count);
+  RM_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (p->count) RM_CUDA_TRY(cudaMemcpy(be.data(), p->d_adj_berr, p->count * sizeof(double), cudaMemcpyDeviceToHost));
+  if (berr) std::copy(be.begin(), be.end(), berr);
+  if (max_berr) {
+    *max_berr = 0.0;
+    for (double v : be) *max_berr = (v != v || *max_berr != *max_berr) ? NAN : std::max(*max_berr, v);
+  }
+  return RM_OK;
+}
+
 int batch_plan_results(BatchPlan* p, double* berr, int32_t* iters, int32_t* flags, rm_batch_report* summary) {
   if (!p) return RM_BAD_ARG;
   const int64_t cnt = p->count;
@@ -826,6 +1149,18 @@ int rm_batch_plan_results(rm_batch_plan* plan, double* h_berr, int32_t* h_iters,
                           rm_batch_report* summary) {
   if (!plan) return RM_BAD_ARG;
   return rm::batch_plan_results(plan->p, h_berr, h_iters, h_flags, summary);
+}
+
+int rm_batch_plan_adjoint(rm_batch_plan* plan, const double* d_a, const double* d_x, const double* d_gx,
+                          double* d_gb, double* d_ga, void* stream) {
+  if (!plan || (plan->p->count > 0 && (!d_a || !d_x || !d_gx || !d_gb))) return RM_BAD_ARG;
+  return rm::batch_plan_adjoint(plan->p, d_a, d_x, d_gx, d_gb, d_ga, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rm_batch_plan_adjoint_results(rm_batch_plan* plan, double* h_berr, double* h_max_berr) {
+  if (!plan) return RM_BAD_ARG;
+  RM_TRY(rm::batch_plan_adjoint_results(plan->p, h_berr, h_max_berr));
+  return rm::take_device_status(nullptr);
 }
 
 int rm_batch_plan_panel_width(const rm_batch_plan* plan, int bucket) {
