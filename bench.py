@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--solve-only", action="store_true",
                    help="only the timed solves (for profiling): no e2e, roofline or CPU legs")
-    p.add_argument("--workload", default="single", choices=["single", "batched"],
+    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint"],
                    help="single: the n=8192 system (the headline); batched: 20,000 uneven systems")
     p.add_argument("--count", type=int, default=20000, help="systems in the batched workload")
     return p.parse_args()
@@ -319,6 +319,69 @@ def run_batched(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+ADJ_METRIC = "gradient solves/s: forward + adjoint (dA, db) of 4096 systems n=64 nrhs=2 on one B200"
+
+
+def run_adjoint(args, rank, world, local):
+    """4096 systems n = 64, k = 2, A = N(0,1)/8 + I, b ~ N(0,1), loss sum(w * x): the forward
+    batched solve and the adjoint kernel (dL/db = A^-T w, dL/dA = -dL/db x^T)."""
+    import torch
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(dev)
+    import rustymath_b200 as rb
+    from rustymath_b200 import _lib
+    lib = _lib.load()
+    batch, n, k = 4096, 64, 2
+    g = torch.Generator(device=dev)
+    g.manual_seed(1 + rank)
+    a = (torch.randn(batch, n, n, generator=g, device=dev, dtype=torch.float64) / 8
+         + torch.eye(n, device=dev, dtype=torch.float64)).reshape(-1).contiguous()
+    b = torch.randn(batch * n * k, generator=g, device=dev, dtype=torch.float64)
+    w = torch.randn(batch * n * k, generator=g, device=dev, dtype=torch.float64)
+    x = torch.empty_like(b)
+    gb = torch.empty_like(b)
+    ga = torch.empty_like(a)
+    plan = rb.BatchPlan([n] * batch, [k] * batch, method="mixed")
+
+    def step():
+        plan.execute(a, b, x)
+        plan.adjoint(a, x, w, gb, ga)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    l0 = lib.rm_launch_count()
+    clocks = ClockSampler(local)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    fwd = bwd = 0.0
+    with clocks:
+        for _ in range(args.steps):
+            e0.record()
+            plan.execute(a, b, x)
+            e1.record()
+            plan.adjoint(a, x, w, gb, ga)
+            e2.record()
+            torch.cuda.synchronize()
+            fwd += e0.elapsed_time(e1) / 1e3
+            bwd += e1.elapsed_time(e2) / 1e3
+    launches = (lib.rm_launch_count() - l0) // args.steps
+    t = (fwd + bwd) / args.steps
+    berr, mx = plan.adjoint_results()
+    da_bytes = batch * n * n * 8
+    line = {"metric": ADJ_METRIC, "value": batch / t, "unit": "systems/s (forward + backward)", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "4096 systems n=64 nrhs=2, A=N(0,1)/8+I, b,w~N(0,1) (torch seeded generator)",
+                       "forward_ms": 1e3 * fwd / args.steps, "adjoint_ms": 1e3 * bwd / args.steps},
+            "adjoint_backward_error_max": mx,
+            "roofline": {"bound": "hbm", "kernel": "batch_adjoint_kernel",
+                         "achieved": (2 * da_bytes) / (bwd / args.steps) / 1e9, "peak": peak_hbm(), "unit": "GB/s",
+                         "frac": (2 * da_bytes) / (bwd / args.steps) / 1e9 / peak_hbm(), "traffic": None,
+                         "note": "algorithmic bytes: A read once (transposed residual) + dA written once"},
+            "gpu_launches": launches, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -328,6 +391,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "batched":
         return run_batched(args, rank, world, local)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
