@@ -134,6 +134,16 @@ int rm_dsolve(int64_t n, const double *d_a, const double *d_b, int64_t k, double
 int rm_dsolve_host(int64_t n, const double *h_a, const double *h_b, int64_t k, double *h_x,
                    const rm_solve_options *opts, rm_solve_report *report);
 
+/* C = A B (row-major float64, no transposes) from int8 tensor-core products: each row of A
+ * and each column of B is scaled by a power of two and cut into `slices` (1..8) signed 7-bit
+ * pieces, the pieces' products of order < slices are formed exactly in int32 and summed in
+ * float64 (the Ozaki split scheme). With 8 slices the error is that of float64 rounding;
+ * fewer trade accuracy for speed (error ~ k 2^-7slices |A||B| by row and column scale).
+ * Inputs must be finite. rustymath's float64 matmul (PlusTimes.inner, core/src/linalg.rs:
+ * 1119-1132) is the native product it stands beside (rm_dgemm). Asynchronous on `stream`. */
+int rm_dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double *d_a, int64_t lda, const double *d_b,
+                   int64_t ldb, double *d_c, int64_t ldc, int slices, void *stream);
+
 /* ---- Batched solves: many small systems of uneven size in one persistent launch.
  * System i is the n[i] x n[i] row-major float64 A at d_a + a_off[i] (items), its right-hand
  * sides the n[i] x k[i] row-major d_b + b_off[i], its solution d_x + x_off[i]; 0 <= n[i] <= 256

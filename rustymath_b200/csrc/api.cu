@@ -286,6 +286,20 @@ int rm_device_count(int* count) {
   return RM_OK;
 }
 
+int rm_dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double* d_a, int64_t lda, const double* d_b, int64_t ldb,
+                   double* d_c, int64_t ldc, int slices, void* stream) {
+  if (m < 0 || n < 0 || k < 0 || slices < 1 || slices > 8) return RM_BAD_ARG;
+  if (m == 0 || n == 0) return RM_OK;
+  if (ldc < n || (k > 0 && (lda < k || ldb < n)) || !d_c || (k > 0 && (!d_a || !d_b))) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  Scratch sc;
+  sc.stream = s;
+  RM_TRY(scratch_alloc(&sc.base, ozaki_scratch_bytes(m, n, k, slices), s));
+  RM_TRY(dgemm_ozaki(m, n, k, d_a, lda, d_b, ldb, d_c, ldc, slices, sc.base, device_status(), s));
+  return RM_OK;
+}
+
 int rm_dgemm(int transa, int transb, int64_t m, int64_t n, int64_t k, double alpha, const double* d_a, int64_t lda,
              const double* d_b, int64_t ldb, double beta, double* d_c, int64_t ldc, void* stream) {
   if (m < 0 || n < 0 || k < 0 || (transa != 0 && transa != 1) || (transb != 0 && transb != 1)) return RM_BAD_ARG;

@@ -100,7 +100,10 @@ unsigned* device_status();
 // Reads and clears the current device's status word (synchronises `stream`); maps bits to
 // an rm status code.
 int take_device_status(cudaStream_t stream);
-int check_device();  // RM_NO_DEVICE without a compute capability 10.x GPU
+int check_device();
+size_t ozaki_scratch_bytes(int64_t m, int64_t n, int64_t k, int s);
+int dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double* a, int64_t lda, const double* b, int64_t ldb,
+                double* c, int64_t ldc, int s, void* scratch, unsigned* status, cudaStream_t stream);  // RM_NO_DEVICE without a compute capability 10.x GPU
 
 // ---------------------------------------------------------------- mixed precision (mixed.cu)
 size_t getrf_lpp_f32_scratch_bytes(int64_t n);

@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib
 from ._lib import NotRegular, SolveOptions, SolveReport, check
 
-__all__ = ["solve", "lu", "Lu", "matmul", "lu_solve", "NotRegular", "SolveReport", "solve_report"]
+__all__ = ["solve", "lu", "Lu", "matmul", "matmul_ozaki", "lu_solve", "NotRegular", "SolveReport", "solve_report"]
 
 _METHODS = {"plain": _lib.RM_METHOD_PLAIN_F64, "f32": _lib.RM_METHOD_F32_IR, "mixed": _lib.RM_METHOD_F32_IR}
 
@@ -372,6 +372,26 @@ def matmul(a, b):
         return c.reshape(n)
     if vb:
         return c.reshape(m)
+    return c
+
+
+def matmul_ozaki(a, b, slices=8):
+    """a @ b for float64 CUDA matrices from int8 tensor-core products (rm_dgemm_ozaki): rows of
+    a and columns of b cut into `slices` 7-bit pieces; 8 slices give float64-level accuracy."""
+    torch = _torch()
+    if not (_is_torch(a) and _is_torch(b) and a.is_cuda and b.is_cuda):
+        raise ValueError("matmul_ozaki works on CUDA tensors")
+    a = a.to(torch.float64).contiguous()
+    b = b.to(torch.float64).contiguous()
+    if a.ndim != 2 or b.ndim != 2 or a.shape[1] != b.shape[0]:
+        raise ValueError("matmul_ozaki needs an m x k and a k x n matrix")
+    m, k = a.shape
+    n = b.shape[1]
+    c = torch.empty((m, n), dtype=torch.float64, device=a.device)
+    if m and n:
+        st = _lib.load().rm_dgemm_ozaki(m, n, k, _ptr(a, True), max(k, 1), _ptr(b, True), max(n, 1), _ptr(c, True),
+                                        n, slices, _stream(True))
+        check(st, "matmul_ozaki")
     return c
 
 
