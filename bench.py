@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--solve-only", action="store_true",
                    help="only the timed solves (for profiling): no e2e, roofline or CPU legs")
-    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint"],
+    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm"],
                    help="single: the n=8192 system (the headline); batched: 20,000 uneven systems")
     p.add_argument("--count", type=int, default=20000, help="systems in the batched workload")
     return p.parse_args()
@@ -382,6 +382,81 @@ def run_adjoint(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+GEMM_METRIC = "FP64-accurate GEMM TFLOP/s at 16384^3: Ozaki int8 split vs native FP64 on one B200"
+
+
+def run_gemm(args, rank, world, local):
+    """C = A B at 16384^3, A and B ~ U(-1,1) with rows of A (columns of B) scaled by 10^U(-3,3):
+    the native FP64 DMMA GEMM (rm_dgemm), the Ozaki int8 split GEMM (rm_dgemm_ozaki, 8 slices)
+    and cuBLAS FP64 (torch.matmul) for reference; errors on 4096 sampled entries against
+    extended-precision dot products (numpy longdouble)."""
+    import torch
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(dev)
+    import rustymath_b200 as rb
+    from rustymath_b200 import _lib
+    lib = _lib.load()
+    n = args.n if args.n != 8192 else 16384
+    g = torch.Generator(device=dev)
+    g.manual_seed(5 + rank)
+    a = (torch.rand(n, n, generator=g, device=dev, dtype=torch.float64) * 2 - 1) * \
+        10.0 ** (torch.rand(n, 1, generator=g, device=dev, dtype=torch.float64) * 6 - 3)
+    b = (torch.rand(n, n, generator=g, device=dev, dtype=torch.float64) * 2 - 1) * \
+        10.0 ** (torch.rand(1, n, generator=g, device=dev, dtype=torch.float64) * 6 - 3)
+    c = torch.empty_like(a)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def native():
+        _lib.check(lib.rm_dgemm(0, 0, n, n, n, 1.0, a.data_ptr(), n, b.data_ptr(), n, 0.0, c.data_ptr(), n, sp), "dgemm")
+
+    def ozaki():
+        _lib.check(lib.rm_dgemm_ozaki(n, n, n, a.data_ptr(), n, b.data_ptr(), n, c.data_ptr(), n, 8, sp), "ozaki")
+
+    def cublas():
+        torch.matmul(a, b, out=c)
+
+    rng = np.random.default_rng(0)
+    rows, cols = rng.integers(0, n, 4096), rng.integers(0, n, 4096)
+    a_s = a[torch.as_tensor(rows, device=dev)].cpu().numpy().astype(np.longdouble)
+    b_s = b[:, torch.as_tensor(cols, device=dev)].cpu().numpy().astype(np.longdouble)
+    ref = np.einsum("ij,ji->i", a_s, b_s)
+    mag = np.einsum("ij,ji->i", np.abs(a_s), np.abs(b_s))
+
+    def timed(fn, steps, clocks=None):
+        for _ in range(max(args.warmup, 3) if steps > 1 else 1):
+            fn()
+        torch.cuda.synchronize()
+        l0 = lib.rm_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with (clocks if clocks is not None else _Null()):
+            e0.record()
+            for _ in range(steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / steps
+        got = c[torch.as_tensor(rows, device=dev), torch.as_tensor(cols, device=dev)].cpu().numpy()
+        err = np.abs(got.astype(np.longdouble) - ref).astype(np.float64) / mag.astype(np.float64)
+        return t, float(err.max()), (lib.rm_launch_count() - l0) // steps
+
+    steps = max(1, min(args.steps, 3))
+    t_nat, e_nat, _ = timed(native, steps)
+    t_cub, e_cub, _ = timed(cublas, steps)
+    clocks = ClockSampler(local)
+    t_oz, e_oz, launches = timed(ozaki, steps, clocks)
+    fl = 2.0 * n ** 3
+    line = {"metric": GEMM_METRIC, "value": fl / t_oz / 1e12, "unit": "TFLOP/s (FP64-equivalent)", "n_gpus": world,
+            "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_oz, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8 slices -> f64", "data": "synthetic",
+            "config": {"workload": f"C=A B at {n}^3, U(-1,1) rows/cols scaled by 10^U(-3,3) (torch seeded)",
+                       "slices": 8},
+            "max_rel_error_vs_|A||B|": {"ozaki": e_oz, "native_fp64": e_nat, "cublas_fp64": e_cub},
+            "native_fp64": {"tflops": fl / t_nat / 1e12, "ms": 1e3 * t_nat},
+            "cublas_fp64": {"tflops": fl / t_cub / 1e12, "ms": 1e3 * t_cub},
+            "gpu_launches": int(launches), "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -393,6 +468,8 @@ def main():
         return run_batched(args, rank, world, local)
     if args.workload == "adjoint":
         return run_adjoint(args, rank, world, local)
+    if args.workload == "gemm":
+        return run_gemm(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
