@@ -47,7 +47,10 @@ extern "C" {
 
 /* Factorization methods for rm_dsolve. */
 #define RM_METHOD_PLAIN_F64 0    /* LU in float64: the drop-in for rustymath's solve */
-#define RM_METHOD_F32_IR 1       /* LU in float32 (tensor-core trailing updates) + float64 refinement */
+#define RM_METHOD_F32_IR 1       /* LU in float32 (tensor-core trailing updates) + float64 refinement;
+                                    when classical refinement stalls, GMRES-IR (restart
+                                    opts->gmres_restart; 0 skips it) with the same factors */
+#define RM_METHOD_GMRES_IR 2     /* (reported in method_used) the answer came from GMRES-IR */
 
 typedef struct rm_solve_options {
   int32_t method;          /* RM_METHOD_* */

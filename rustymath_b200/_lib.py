@@ -10,7 +10,7 @@ LIB_PATH = os.path.join(HERE, "librm_cuda.so")
 
 RM_OK, RM_BAD_ARG, RM_NOT_REGULAR, RM_CUDA_ERROR = 0, 1, 2, 3
 RM_TIMEOUT, RM_NO_CONVERGENCE, RM_NO_DEVICE, RM_OUT_OF_MEMORY = 4, 5, 6, 7
-RM_METHOD_PLAIN_F64, RM_METHOD_F32_IR = 0, 1
+RM_METHOD_PLAIN_F64, RM_METHOD_F32_IR, RM_METHOD_GMRES_IR = 0, 1, 2
 
 _i32, _i64, _f64, _p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 

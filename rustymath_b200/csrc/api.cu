@@ -637,7 +637,7 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
   const double tol = opts->tolerance > 0.0 ? opts->tolerance : (double)n * 0x1.0p-53;
   const int max_it = opts->max_iterations > 0 ? opts->max_iterations : 30;
   int iterations = 0;
-  bool converged = false;
+  bool converged = false, gmres = false, timed_out = false;
   double berr_h = 0.0;
   {
     Arena ar;
@@ -675,7 +675,10 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
       RM_CUDA_TRY(cudaMemcpyAsync(&berr_h, sc.at<double>(oberr), sizeof berr_h, cudaMemcpyDeviceToHost, s));
       const int dst = take_device_status(s);  // synchronises
       if (dst != RM_OK && dst != RM_TIMEOUT) return dst;
-      if (dst == RM_TIMEOUT) break;
+      if (dst == RM_TIMEOUT) {
+        timed_out = true;
+        break;
+      }
       if (berr_h <= tol) {
         converged = true;
         break;
@@ -689,12 +692,30 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
       tr.mark("solve");
       ++iterations;
     }
+    if (!converged && !timed_out && opts->gmres_restart > 0 && berr_h == berr_h) {
+      // classical refinement stalled: GMRES-IR with the same float32 factors as preconditioner
+      Scratch gs;
+      gs.stream = s;
+      RM_TRY(scratch_alloc(&gs.base, gmres_scratch_bytes(n, k, opts->gmres_restart), s));
+      Precond pc{f, ldf, n, perm, sc.at<float>(odinv), pre, c, sc.at<void>(otr), st};
+      int outer = 0;
+      double berr_g = INFINITY;
+      RM_TRY(gmres_ir(d_a, n, d_b, k, d_x, pc, opts->gmres_restart, max_it, tol, &berr_g, &outer, gs.base,
+                      sc.at<double>(orr), sc.at<double>(onorm), sc.at<double>(oberr), s));
+      tr.mark("gmres_ir");
+      iterations += outer;
+      if (berr_g <= tol) {
+        converged = true;
+        gmres = true;
+        berr_h = berr_g;
+      }
+    }
   }
   if (converged) {
     if (report) {
       report->backward_error = berr_h;
       report->iterations = iterations;
-      report->method_used = RM_METHOD_F32_IR;
+      report->method_used = gmres ? RM_METHOD_GMRES_IR : RM_METHOD_F32_IR;
       report->fell_back = 0;
       report->regular = 1;
     }

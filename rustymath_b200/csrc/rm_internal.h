@@ -126,6 +126,27 @@ int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, f
 int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv, const float* pre, float* x,
                        int64_t ldx, int64_t k, void* scratch, unsigned* status, cudaStream_t stream);
 
+// z = (LU)^-1 P y in float64 through the float32 factors of the mixed solve (y may be z)
+struct Precond {
+  const float* f;
+  int64_t ldf, n;
+  const int* perm;
+  const float* dinv;
+  const float* pre;
+  float* c;  // n x k float32 work
+  void* trsv;
+  unsigned* st;
+  int apply(const double* y, double* z, int64_t k, cudaStream_t s) const {
+    RM_TRY(gather_f32(y, k, perm, n, k, c, k, s));
+    RM_TRY(lu_solve_f32_nopiv(f, ldf, n, dinv, pre, c, k, k, trsv, st, s));
+    return accumulate_f64(c, k, n, k, z, k, true, s);
+  }
+};
+size_t gmres_scratch_bytes(int64_t n, int64_t k, int restart);
+int gmres_ir(const double* a, int64_t n, const double* b, int64_t k, double* x, const Precond& pc, int restart,
+             int max_outer, double tol, double* berr_out, int* outer_out, void* scratch, double* r, double* norms,
+             double* berr_dev, cudaStream_t s);
+
 // ---------------------------------------------------------------- helpers (api.cu)
 int64_t round_up(int64_t x, int64_t m);
 // Stream-ordered scratch allocation from the device's default pool.

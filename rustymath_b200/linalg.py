@@ -67,11 +67,11 @@ def _empty(shape, like, device, dtype=np.float64):
     return np.empty(shape, dtype=dtype)
 
 
-def _options(method, max_iterations=30, tolerance=0.0, fallback=True):
+def _options(method, max_iterations=30, tolerance=0.0, fallback=True, gmres_restart=20):
     o = SolveOptions()
     o.method = _METHODS[method]
     o.max_iterations = max_iterations
-    o.gmres_restart = 20
+    o.gmres_restart = gmres_restart
     o.fallback = 1 if fallback else 0
     o.tolerance = tolerance
     return o

@@ -32,7 +32,7 @@ def test_mixed_meets_the_fp64_bar(rb, n, k, kappa):
     a, b = conditioned(n, k, kappa, n + k)
     x, reps = rb.solve_report(a, b, method="mixed")
     rep = reps[0]
-    assert rep.method_used == 1 and rep.fell_back == 0, "refinement converged without falling back"
+    assert rep.method_used == 1 and rep.fell_back == 0, "classical refinement converged"
     assert rep.iterations <= 5
     assert O.backward_error(a, x, b) <= n * 2.0 ** -53
     xo = O.solve(a, b)
@@ -47,14 +47,40 @@ def test_mixed_device_tensors(rb):
     assert O.backward_error(a, x.cpu().numpy(), b) <= n * 2.0 ** -53
 
 
-def test_mixed_falls_back_when_refinement_stalls(rb):
-    """kappa = 1e12 is beyond float32 factors' reach (kappa * u >> 1): refinement stalls and
-    the plain float64 LU answers, as the report says."""
+def test_mixed_beyond_float32_reach(rb):
+    """kappa = 1e12 is beyond float32 factors' reach (kappa * u >> 1): classical refinement
+    stalls; GMRES-IR or, failing it, the plain float64 LU answers, as the report says."""
     n, k = 300, 2
     a, b = conditioned(n, k, 1e12, 5)
     x, reps = rb.solve_report(a, b, method="mixed")
-    assert reps[0].fell_back == 1 and reps[0].method_used == 0
+    assert reps[0].method_used in (0, 2)
+    assert reps[0].fell_back == (1 if reps[0].method_used == 0 else 0)
     assert O.backward_error(a, x, b) <= n * 2.0 ** -53
+
+
+@pytest.mark.parametrize("kappa,restart", [(3e7, 20), (1e8, 60)])
+def test_gmres_ir_where_classical_refinement_stalls(rb, kappa, restart):
+    """kappa * u_f near or above 1: classical refinement with float32 factors stalls, while
+    flexible GMRES right-preconditioned by the same factors converges (GMRES-IR); at 1e8 it
+    needs a longer restart cycle."""
+    import ctypes
+    from rustymath_b200 import _lib
+    n, k = 401, 3  # odd n: the float64 products take a padded copy of A
+    a, b = conditioned(n, k, kappa, 11)
+    lib = _lib.load()
+    x = np.zeros((n, k))
+    opts = rb.linalg._options("mixed", gmres_restart=restart)
+    rep = _lib.SolveReport()
+    st = lib.rm_dsolve_host(n, a.ctypes.data, b.ctypes.data, k, x.ctypes.data, ctypes.byref(opts), ctypes.byref(rep))
+    assert st == 0 and rep.method_used == _lib.RM_METHOD_GMRES_IR and rep.fell_back == 0
+    assert O.backward_error(a, x, b) <= n * 2.0 ** -53
+    # with GMRES-IR switched off, the float64 fallback answers instead
+    x2 = np.zeros((n, k))
+    opts = rb.linalg._options("mixed", gmres_restart=0)
+    st = lib.rm_dsolve_host(n, a.ctypes.data, b.ctypes.data, k, x2.ctypes.data, ctypes.byref(opts),
+                            ctypes.byref(rep))
+    assert st == 0 and rep.fell_back == 1 and rep.method_used == 0
+    assert O.backward_error(a, x2, b) <= n * 2.0 ** -53
 
 
 def test_mixed_singular_matrix_is_not_regular(rb):
