@@ -137,6 +137,23 @@ int rm_dsolve(int64_t n, const double *d_a, const double *d_b, int64_t k, double
 int rm_dsolve_host(int64_t n, const double *h_a, const double *h_b, int64_t k, double *h_x,
                    const rm_solve_options *opts, rm_solve_report *report);
 
+/* X = op(A)^-1 X (side RM_LEFT, A m x m) or X op(A)^-1 (RM_RIGHT, A n x n) in place for the
+ * row-major m x n X, with alpha = 1: the shape of Accelerated::xtrsm (core/src/linalg/
+ * accelerate.rs:215, 269-275), reached from Tiled::triangular through accelerate::triangular
+ * (accelerate.rs:67-74). The codes are CBLAS's, as the reference passes them: side 141/142,
+ * uplo 121 (upper) / 122 (lower), trans 111/112, diag 131 (non-unit) / 132 (unit); row-major
+ * storage (CBLAS order 101) is implied. Synchronises on `stream`. */
+#define RM_LEFT 141
+#define RM_RIGHT 142
+#define RM_UPPER 121
+#define RM_LOWER 122
+#define RM_CBLAS_NO_TRANS 111
+#define RM_CBLAS_TRANS 112
+#define RM_NON_UNIT 131
+#define RM_UNIT 132
+int rm_dtrsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, const double *d_a, int64_t lda,
+             double *d_x, int64_t ldx, void *stream);
+
 /* C = A B (row-major float64, no transposes) from int8 tensor-core products: each row of A
  * and each column of B is scaled by a power of two and cut into `slices` (1..8) signed 7-bit
  * pieces, the pieces' products of order < slices are formed exactly in int32 and summed in

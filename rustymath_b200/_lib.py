@@ -62,6 +62,8 @@ SIGNATURES = {
     "rm_batch_plan_results": (ctypes.c_int, [_p, _p, _p, _p, ctypes.POINTER(BatchReport)]),
     "rm_batch_plan_panel_width": (ctypes.c_int, [_p, ctypes.c_int]),
     "rm_batch_plan_adjoint": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p]),
+    "rm_dtrsm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _i64, _p, _i64, _p,
+                                _i64, _p]),
     "rm_dgemm_ozaki": (ctypes.c_int, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, ctypes.c_int, _p]),
     "rm_batch_plan_adjoint_results": (ctypes.c_int, [_p, _p, _p]),
     "rm_batch_plan_destroy": (ctypes.c_int, [_p]),

@@ -286,6 +286,26 @@ int rm_device_count(int* count) {
   return RM_OK;
 }
 
+int rm_dtrsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, const double* d_a, int64_t lda,
+             double* d_x, int64_t ldx, void* stream) {
+  if ((side != RM_LEFT && side != RM_RIGHT) || (uplo != RM_UPPER && uplo != RM_LOWER) ||
+      (trans != RM_CBLAS_NO_TRANS && trans != RM_CBLAS_TRANS) || (diag != RM_NON_UNIT && diag != RM_UNIT) || m < 0 ||
+      n < 0)
+    return RM_BAD_ARG;
+  if (m == 0 || n == 0) return RM_OK;
+  const bool right = side == RM_RIGHT;
+  const int64_t order = right ? n : m;
+  if (lda < order || ldx < n || !d_a || !d_x) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s = as_stream(stream);
+  Scratch sc;
+  sc.stream = s;
+  RM_TRY(scratch_alloc(&sc.base, trsm_f64_scratch_bytes(order, m, n, right), s));
+  RM_TRY(trsm_f64(right, uplo == RM_LOWER, trans == RM_CBLAS_TRANS, diag == RM_UNIT, m, n, d_a, lda, d_x, ldx, sc.base,
+                  device_status(), s));
+  return take_device_status(s);
+}
+
 int rm_dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double* d_a, int64_t lda, const double* d_b, int64_t ldb,
                    double* d_c, int64_t ldc, int slices, void* stream) {
   if (m < 0 || n < 0 || k < 0 || slices < 1 || slices > 8) return RM_BAD_ARG;

@@ -430,6 +430,59 @@ int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const i
   return RM_OK;
 }
 
+// ------------------------------------------------------------------ a triangular solve (TRSM)
+
+size_t trsm_f64_scratch_bytes(int64_t order, int64_t m, int64_t n, bool right) {
+  const int64_t nblk = (order + kTB64 - 1) / kTB64, cols = right ? m : n;
+  return (diag_blocks_bytes_max(order) + 255) / 256 * 256 +
+         ((size_t)(nblk + 1) * sizeof(int) * (size_t)((cols + kKC - 1) / kKC) + 255) / 256 * 256 +
+         (right ? (size_t)m * n * sizeof(double) : 0) + 256;
+}
+
+// x = op(A)^-1 x (left, A m x m) or x op(A)^-1 (right, A n x n) for the row-major m x n x, A
+// triangular (lower or upper, unit or not), op(A) = A or A^T: the block-chained solve of
+// getrs on one triangle. A right-side solve is a left-side one on x^T with op(A)^T.
+int trsm_f64(bool right, bool lower, bool trans, bool unit, int64_t m, int64_t n, const double* a, int64_t lda,
+             double* x, int64_t ldx, void* scratch, unsigned* status, cudaStream_t stream) {
+  if (m == 0 || n == 0) return RM_OK;
+  const int64_t order = right ? n : m, cols = right ? m : n;
+  // the solved triangle T: item (i, j) at a[i*lda + j] (row view) or a[j*lda + i] (column view)
+  const bool colview = right ? !trans : trans;
+  const bool low = colview ? !lower : lower;
+  const int nblk = (int)((order + kTB64 - 1) / kTB64);
+  double* dinv = reinterpret_cast<double*>(scratch);
+  int* flags = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + (diag_blocks_bytes_max(order) + 255) / 256 * 256);
+  const int chunks = (int)((cols + kKC - 1) / kKC);
+  double* xt = reinterpret_cast<double*>(reinterpret_cast<char*>(flags) +
+                                         ((size_t)(nblk + 1) * sizeof(int) * chunks + 255) / 256 * 256);
+  RM_TRY(invert_diag_blocks_f64(a, lda, colview, order, dinv, unit, unit, stream));
+  RM_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)(nblk + 1) * sizeof(int) * chunks, stream));
+  double* y = x;
+  int64_t ldy = ldx;
+  if (right) {  // x^T (n x m) row-major
+    RM_TRY(transpose_f64(x, ldx, m, n, xt, m, stream));
+    y = xt;
+    ldy = m;
+  }
+  const int no = (int)order;
+  for (int ch = 0; ch < chunks; ++ch) {
+    const int kc = (int)std::min<int64_t>(kKC, cols - (int64_t)ch * kKC);
+    int* f = flags + (size_t)ch * (nblk + 1);
+    double* yc = y + ch * kKC;
+    if (colview) {
+      if (low) RM_TRY((launch_trsv<double, true, true, kTB64>(a, lda, no, dinv, yc, ldy, kc, f, f + nblk, status, stream)));
+      else RM_TRY((launch_trsv<double, false, true, kTB64>(a, lda, no, dinv, yc, ldy, kc, f, f + nblk, status, stream)));
+    } else {
+      if (low) RM_TRY((launch_trsv<double, true, false, kTB64>(a, lda, no, dinv, yc, ldy, kc, f, f + nblk, status, stream)));
+      else RM_TRY((launch_trsv<double, false, false, kTB64>(a, lda, no, dinv, yc, ldy, kc, f, f + nblk, status, stream)));
+    }
+  }
+  if (right) {
+    RM_TRY(transpose_f64(xt, m, n, m, x, ldx, stream));
+  }
+  return RM_OK;
+}
+
 // ------------------------------------------------------------------ float32, no pivoting
 
 size_t diag_blocks_f32_bytes(int64_t n) {

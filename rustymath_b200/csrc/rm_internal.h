@@ -101,6 +101,9 @@ unsigned* device_status();
 // an rm status code.
 int take_device_status(cudaStream_t stream);
 int check_device();
+size_t trsm_f64_scratch_bytes(int64_t order, int64_t m, int64_t n, bool right);
+int trsm_f64(bool right, bool lower, bool trans, bool unit, int64_t m, int64_t n, const double* a, int64_t lda,
+             double* x, int64_t ldx, void* scratch, unsigned* status, cudaStream_t stream);
 size_t ozaki_scratch_bytes(int64_t m, int64_t n, int64_t k, int s);
 int dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double* a, int64_t lda, const double* b, int64_t ldb,
                 double* c, int64_t ldc, int s, void* scratch, unsigned* status, cudaStream_t stream);  // RM_NO_DEVICE without a compute capability 10.x GPU
