@@ -160,6 +160,32 @@ def time_dgemm_update(torch, lib, dev, n, k=128, reps=10):
     return 2.0 * m * m * k / t / 1e12, t
 
 
+def time_sgemm_update(torch, lib, dev, n, k=128, reps=10):
+    """One launch of the mixed LU's dominant tensor-core kernel: the rank-128 trailing update
+    A22 -= L21 U12 (3xTF32 tcgen05 GEMM, beta = 1) at the first step's size. It is HBM-bound:
+    its algorithmic bytes are C read and written once (8 bytes per item) plus the two panels."""
+    m = n - k
+    a = torch.randn(m, k, device=dev, dtype=torch.float32)
+    b = torch.randn(m, k, device=dev, dtype=torch.float32)
+    c = torch.randn(m, m, device=dev, dtype=torch.float32)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def go():
+        return lib.rm_sgemm_tc(3, 1, m, m, k, -1.0, a.data_ptr(), k, b.data_ptr(), k, 1.0, c.data_ptr(), m, s)
+
+    for _ in range(3):
+        assert go() == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        go()
+    e1.record()
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    bytes_ = m * m * 8 + 2 * m * k * 4
+    return bytes_ / t / 1e9, t, bytes_, 3 * 2.0 * m * m * k / t / 1e12
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -563,13 +589,21 @@ def main():
            "d2h_bytes_per_step": n * k * 8, "api": "rm_dsolve_host (pinned host buffers)"}
 
     if rank == 0:
-        # ---- roofline of the dominant kernel (the FP64 DMMA trailing update)
+        # ---- roofline of the mixed path's dominant tensor-core kernel (the 3xTF32 rank-128
+        # update, HBM-bound) and, beside it, the plain path's FP64 DMMA update
+        gbs, t_upd, bytes_upd, tf32_tflops = time_sgemm_update(torch, lib, dev, n)
+        roofline = {"bound": "hbm", "kernel": "sgemm_tc_kernel<3,TMA> rank-128 update m=n=8064 k=128 (3xTF32)",
+                    "achieved": gbs, "peak": peak_hbm(), "unit": "GB/s", "frac": gbs / peak_hbm(),
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)",
+                    "bytes_per_launch": bytes_upd, "launch_us": 1e6 * t_upd, "tf32_tflops": tf32_tflops,
+                    "traffic": None}
         peak64 = gemm_peak_f64(torch, dev)
         achieved, t_launch = time_dgemm_update(torch, lib, dev, n)
-        roofline = {"bound": "tensor", "kernel": "dgemm_kernel<128x128> rank-128 update m=n=8064 k=128",
-                    "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
-                    "peak_source": "measured cuBLAS FP64 GEMM 8192^3 in this run (no FP64 figure in MEASURED_PEAKS.json)",
-                    "traffic": None}
+        roofline["plain_path_dgemm"] = {"bound": "tensor", "kernel": "dgemm_kernel<128x128> rank-128 update",
+                                        "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                                        "frac": achieved / peak64,
+                                        "peak_source": "cuBLAS FP64 GEMM 8192^3 in this run (no FP64 figure in "
+                                                       "MEASURED_PEAKS.json)"}
         cpu = None
         if not args.no_cpu_baseline:
             cpu, x_cpu = cpu_baseline(a_h.numpy(), b_h.numpy())
