@@ -506,6 +506,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import rustymath_b200 as rb
     from rustymath_b200 import _lib
+    from rustymath_b200.parallel import max_over_ranks
     lib = _lib.load()
 
     n, k = args.n, args.nrhs
@@ -540,11 +541,7 @@ def main():
             e1.record()
             torch.cuda.synchronize()
         launches = (lib.rm_launch_count() - launches0) // max(steps, 1)
-        elapsed = e0.elapsed_time(e1) / 1e3
-        if world > 1:
-            t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            elapsed = float(t.item())
+        elapsed = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         return elapsed, rep, launches
 
     # the plain float64 LU first (the comparison arm), then the headline method
