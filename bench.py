@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--solve-only", action="store_true",
                    help="only the timed solves (for profiling): no e2e, roofline or CPU legs")
-    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm"],
+    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm", "update"],
                    help="single: the n=8192 system (the headline); batched: 20,000 uneven systems")
     p.add_argument("--count", type=int, default=20000, help="systems in the batched workload")
     return p.parse_args()
@@ -483,6 +483,20 @@ def run_gemm(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_update(args, rank, world, local):
+    """The headline roofline's kernel alone: the mixed LU's first rank-128 trailing update
+    (3xTF32 tcgen05, m = n = n - 128, k = 128, beta = 1), timed by CUDA events (for profiling)."""
+    import torch
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(dev)
+    from rustymath_b200 import _lib
+    lib = _lib.load()
+    gbs, t, bytes_, tf = time_sgemm_update(torch, lib, dev, args.n, reps=max(args.steps, 1))
+    print(json.dumps({"workload": f"rank-128 update m=n={args.n - 128} k=128 (3xTF32)", "achieved_gbs": gbs,
+                      "peak_gbs": peak_hbm(), "frac": gbs / peak_hbm(), "launch_us": 1e6 * t,
+                      "bytes_per_launch": bytes_, "tf32_tflops": tf}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -496,6 +510,8 @@ def main():
         return run_adjoint(args, rank, world, local)
     if args.workload == "gemm":
         return run_gemm(args, rank, world, local)
+    if args.workload == "update":
+        return run_update(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
@@ -593,7 +609,9 @@ def main():
                     "achieved": gbs, "peak": peak_hbm(), "unit": "GB/s", "frac": gbs / peak_hbm(),
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)",
                     "bytes_per_launch": bytes_upd, "launch_us": 1e6 * t_upd, "tf32_tflops": tf32_tflops,
-                    "traffic": None}
+                    "traffic": 268.48e6 + 200.21e6,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch at full size "
+                                      "(bench.py --workload update, the 4th launch)"}
         peak64 = gemm_peak_f64(torch, dev)
         achieved, t_launch = time_dgemm_update(torch, lib, dev, n)
         roofline["plain_path_dgemm"] = {"bound": "tensor", "kernel": "dgemm_kernel<128x128> rank-128 update",

@@ -153,6 +153,8 @@ int rm_dsolve_host(int64_t n, const double *h_a, const double *h_b, int64_t k, d
 #define RM_UNIT 132
 int rm_dtrsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, const double *d_a, int64_t lda,
              double *d_x, int64_t ldx, void *stream);
+int rm_dtrsm_host(int side, int uplo, int trans, int diag, int64_t m, int64_t n, const double *h_a, int64_t lda,
+                  double *h_x, int64_t ldx);
 
 /* C = A B (row-major float64, no transposes) from int8 tensor-core products: each row of A
  * and each column of B is scaled by a power of two and cut into `slices` (1..8) signed 7-bit
@@ -163,6 +165,8 @@ int rm_dtrsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, cons
  * 1119-1132) is the native product it stands beside (rm_dgemm). Asynchronous on `stream`. */
 int rm_dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double *d_a, int64_t lda, const double *d_b,
                    int64_t ldb, double *d_c, int64_t ldc, int slices, void *stream);
+int rm_dgemm_ozaki_host(int64_t m, int64_t n, int64_t k, const double *h_a, int64_t lda, const double *h_b,
+                        int64_t ldb, double *h_c, int64_t ldc, int slices);
 
 /* ---- Batched solves: many small systems of uneven size in one persistent launch.
  * System i is the n[i] x n[i] row-major float64 A at d_a + a_off[i] (items), its right-hand
@@ -221,6 +225,10 @@ int rm_batch_plan_destroy(rm_batch_plan *plan);
 int rm_dsolve_batched(int64_t count, const int64_t *h_n, const int64_t *h_k, const int64_t *h_a_off,
                       const int64_t *h_b_off, const int64_t *h_x_off, const double *d_a, const double *d_b,
                       double *d_x, const rm_solve_options *opts, rm_batch_report *report, void *stream);
+/* The same with host A, B and X (the host-pointer form of every batched entry point above). */
+int rm_dsolve_batched_host(int64_t count, const int64_t *h_n, const int64_t *h_k, const int64_t *h_a_off,
+                           const int64_t *h_b_off, const int64_t *h_x_off, const double *h_a, const double *h_b,
+                           double *h_x, const rm_solve_options *opts, rm_batch_report *report);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,11 @@ SIGNATURES = {
     "rm_batch_plan_adjoint": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p]),
     "rm_dtrsm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _i64, _p, _i64, _p,
                                 _i64, _p]),
+    "rm_dtrsm_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _i64, _p, _i64,
+                                     _p, _i64]),
+    "rm_dgemm_ozaki_host": (ctypes.c_int, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, ctypes.c_int]),
+    "rm_dsolve_batched_host": (ctypes.c_int, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.POINTER(SolveOptions),
+                                              ctypes.POINTER(BatchReport)]),
     "rm_dgemm_ozaki": (ctypes.c_int, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, ctypes.c_int, _p]),
     "rm_batch_plan_adjoint_results": (ctypes.c_int, [_p, _p, _p]),
     "rm_batch_plan_destroy": (ctypes.c_int, [_p]),

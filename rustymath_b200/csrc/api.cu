@@ -809,4 +809,117 @@ int rm_dsolve_host(int64_t n, const double* h_a, const double* h_b, int64_t k, d
   return st;
 }
 
+// Host-pointer forms of rm_dtrsm, rm_dgemm_ozaki and rm_dsolve_batched: copy in on a stream of
+// their own, run the device form, copy back, synchronise.
+namespace {
+struct HostCall {
+  cudaStream_t s = nullptr;
+  Scratch sc;
+  int st = RM_OK;
+  explicit HostCall(size_t bytes) {
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      st = RM_CUDA_ERROR;
+      return;
+    }
+    sc.stream = s;
+    st = scratch_alloc(&sc.base, bytes, s);
+  }
+  int copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (st != RM_OK || bytes == 0) return st;
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s);
+    if (e != cudaSuccess) {
+      set_last_error(e, "copy", __FILE__, __LINE__);
+      st = RM_CUDA_ERROR;
+    }
+    return st;
+  }
+  int finish() {
+    if (!s) return st;
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (st == RM_OK && e != cudaSuccess) {
+      set_last_error(e, "sync", __FILE__, __LINE__);
+      st = RM_CUDA_ERROR;
+    }
+    return st;
+  }
+  ~HostCall() {
+    if (s) {
+      scratch_free(sc.base, s);
+      sc.base = nullptr;
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+}  // namespace
+
+int rm_dtrsm_host(int side, int uplo, int trans, int diag, int64_t m, int64_t n, const double* h_a, int64_t lda,
+                  double* h_x, int64_t ldx) {
+  if (m < 0 || n < 0) return RM_BAD_ARG;
+  if (m == 0 || n == 0) return rm_dtrsm(side, uplo, trans, diag, m, n, h_a, lda, h_x, ldx, nullptr);
+  const int64_t order = side == RM_RIGHT ? n : m;
+  if (!h_a || !h_x || lda < order || ldx < n) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  Arena ar;
+  const size_t oa = ar.add((size_t)order * lda * 8), ox = ar.add((size_t)m * ldx * 8);
+  HostCall hc(ar.total);
+  double* a = hc.sc.at<double>(oa);
+  double* x = hc.sc.at<double>(ox);
+  hc.copy(a, h_a, (size_t)order * lda * 8, cudaMemcpyHostToDevice);
+  hc.copy(x, h_x, (size_t)m * ldx * 8, cudaMemcpyHostToDevice);
+  if (hc.st == RM_OK) hc.st = rm_dtrsm(side, uplo, trans, diag, m, n, a, lda, x, ldx, hc.s);
+  hc.copy(h_x, x, (size_t)m * ldx * 8, cudaMemcpyDeviceToHost);
+  return hc.finish();
+}
+
+int rm_dgemm_ozaki_host(int64_t m, int64_t n, int64_t k, const double* h_a, int64_t lda, const double* h_b,
+                        int64_t ldb, double* h_c, int64_t ldc, int slices) {
+  if (m < 0 || n < 0 || k < 0) return RM_BAD_ARG;
+  if (m == 0 || n == 0) return RM_OK;
+  if (!h_c || ldc < n || (k > 0 && (!h_a || !h_b || lda < k || ldb < n))) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  Arena ar;
+  const size_t oa = ar.add((size_t)m * std::max<int64_t>(lda, 1) * 8), ob = ar.add((size_t)k * ldb * 8);
+  const size_t oc = ar.add((size_t)m * ldc * 8);
+  HostCall hc(ar.total);
+  hc.copy(hc.sc.at<double>(oa), h_a, (size_t)m * lda * 8 * (k > 0), cudaMemcpyHostToDevice);
+  hc.copy(hc.sc.at<double>(ob), h_b, (size_t)k * ldb * 8, cudaMemcpyHostToDevice);
+  if (hc.st == RM_OK)
+    hc.st = rm_dgemm_ozaki(m, n, k, hc.sc.at<double>(oa), std::max<int64_t>(lda, 1), hc.sc.at<double>(ob),
+                           std::max<int64_t>(ldb, 1), hc.sc.at<double>(oc), ldc, slices, hc.s);
+  hc.copy(h_c, hc.sc.at<double>(oc), (size_t)m * ldc * 8, cudaMemcpyDeviceToHost);
+  return hc.finish();
+}
+
+int rm_dsolve_batched_host(int64_t count, const int64_t* h_n, const int64_t* h_k, const int64_t* h_a_off,
+                           const int64_t* h_b_off, const int64_t* h_x_off, const double* h_a, const double* h_b,
+                           double* h_x, const rm_solve_options* opts, rm_batch_report* report) {
+  if (count < 0 || (count > 0 && (!h_n || !h_k || !h_a_off || !h_b_off || !h_x_off))) return RM_BAD_ARG;
+  int64_t na = 0, nb = 0, nx = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    if (h_n[i] < 0 || h_k[i] < 0 || h_a_off[i] < 0 || h_b_off[i] < 0 || h_x_off[i] < 0) return RM_BAD_ARG;
+    na = std::max(na, h_a_off[i] + h_n[i] * h_n[i]);
+    nb = std::max(nb, h_b_off[i] + h_n[i] * h_k[i]);
+    nx = std::max(nx, h_x_off[i] + h_n[i] * h_k[i]);
+  }
+  if ((na && !h_a) || (nb && !h_b) || (nx && !h_x)) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  Arena ar;
+  const size_t oa = ar.add((size_t)na * 8 + 8), ob = ar.add((size_t)nb * 8 + 8), ox = ar.add((size_t)nx * 8 + 8);
+  HostCall hc(ar.total);
+  hc.copy(hc.sc.at<double>(oa), h_a, (size_t)na * 8, cudaMemcpyHostToDevice);
+  hc.copy(hc.sc.at<double>(ob), h_b, (size_t)nb * 8, cudaMemcpyHostToDevice);
+  hc.copy(hc.sc.at<double>(ox), h_x, (size_t)nx * 8, cudaMemcpyHostToDevice);  // x's untouched items survive
+  if (hc.st == RM_OK)
+    hc.st = rm_dsolve_batched(count, h_n, h_k, h_a_off, h_b_off, h_x_off, hc.sc.at<double>(oa), hc.sc.at<double>(ob),
+                              hc.sc.at<double>(ox), opts, report, hc.s);
+  if (hc.st == RM_OK || hc.st == RM_NO_CONVERGENCE) {
+    const int keep = hc.st;
+    hc.st = RM_OK;
+    hc.copy(h_x, hc.sc.at<double>(ox), (size_t)nx * 8, cudaMemcpyDeviceToHost);
+    if (hc.finish() == RM_OK) return keep;
+  }
+  return hc.finish();
+}
+
 }  // extern "C"

@@ -402,6 +402,26 @@ __global__ void iota32_kernel(int* p, int64_t n) {
     p[i] = (int)i;
 }
 
+// The side stream and the two events of the look-ahead; released when the factorization returns
+// (work still queued on the side stream completes first).
+struct LookAhead {
+  cudaStream_t side = nullptr;
+  cudaEvent_t next_done = nullptr, rest_done = nullptr;
+  int open() {
+    RM_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&next_done, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&rest_done, cudaEventDisableTiming));
+    // rest_done starts out complete, so the first wait on it passes
+    RM_CUDA_TRY(cudaEventRecord(rest_done, side));
+    return RM_OK;
+  }
+  ~LookAhead() {
+    if (next_done) cudaEventDestroy(next_done);
+    if (rest_done) cudaEventDestroy(rest_done);
+    if (side) cudaStreamDestroy(side);
+  }
+};
+
 size_t getrf_lpp_f32_scratch_bytes(int64_t n) {
   return (2 * (size_t)kLppCols * kLppCols + 2 * (size_t)n * kLppCols) * sizeof(float) + kLppRows * sizeof(int) +
          2048;
@@ -422,6 +442,12 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
   }
   iota32_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 1024), 256, 0, stream>>>(perm, n);
   RM_LAUNCHED();
+  // Look-ahead: the next panel's 128 columns of each trailing update go first, on `stream`;
+  // the rest of the update runs on a side stream on all SMs but one while the next panel
+  // (one CTA) factors on the SM left free; the panel's row permutation then waits for it.
+  LookAhead la;
+  const bool ahead = n >= 1024 && device_sm_count() > 1;
+  if (ahead) RM_TRY(la.open());
   const int ni = (int)n;
   for (int J0 = 0; J0 < ni; J0 += kLppCols) {
     const int nb = std::min(kLppCols, ni - J0);
@@ -430,6 +456,7 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
     const int rest = ni - J1;
     lpp_panel_kernel<<<1, kLppThreads, kLppSmem, stream>>>(a, lda, J0, nb, T, linv, uinvt, plocal, status);
     RM_LAUNCHED();
+    if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
     const int chunks = (J0 + kApplyCols - 1) / kApplyCols + (rest + kApplyCols - 1) / kApplyCols;
     lpp_apply_kernel<<<std::max(chunks, 1), 256, 0, stream>>>(a, lda, ni, J0, J1, T, plocal, a12t, perm);
     RM_LAUNCHED();
@@ -444,10 +471,24 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
       float* a21b = a + (int64_t)(J0 + T) * lda + J0;
       RM_TRY(sgemm_tc(3, below, nb, nb, 1.0f, a21b, lda, uinvt, kLppCols, 0.0f, a21b, lda, status, stream));
     }
-    // A22 -= L21 U12
-    RM_TRY(sgemm_tc(3, rest, rest, nb, -1.0f, a + (int64_t)J1 * lda + J0, lda, u12t, kLppCols, 1.0f,
-                    a + (int64_t)J1 * lda + J1, lda, status, stream));
+    // A22 -= L21 U12: the next panel's columns, then the rest
+    const float* l21 = a + (int64_t)J1 * lda + J0;
+    float* a22 = a + (int64_t)J1 * lda + J1;
+    if (!ahead) {
+      RM_TRY(sgemm_tc(3, rest, rest, nb, -1.0f, l21, lda, u12t, kLppCols, 1.0f, a22, lda, status, stream));
+      continue;
+    }
+    const int nn = std::min(kLppCols, rest);
+    RM_TRY(sgemm_tc(3, rest, nn, nb, -1.0f, l21, lda, u12t, kLppCols, 1.0f, a22, lda, status, stream));
+    if (rest > nn) {
+      RM_CUDA_TRY(cudaEventRecord(la.next_done, stream));
+      RM_CUDA_TRY(cudaStreamWaitEvent(la.side, la.next_done, 0));
+      RM_TRY(sgemm_tc(3, rest, rest - nn, nb, -1.0f, l21, lda, u12t + (size_t)nn * kLppCols, kLppCols, 1.0f, a22 + nn,
+                      lda, status, la.side, nullptr, 0, device_sm_count() - 1));
+      RM_CUDA_TRY(cudaEventRecord(la.rest_done, la.side));
+    }
   }
+  if (ahead) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
   return RM_OK;
 }
 

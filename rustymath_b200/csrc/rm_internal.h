@@ -20,9 +20,10 @@ int scale_device(double* c, int64_t ldc, int64_t m, int64_t n, double beta, cuda
 // C = alpha A B^T + beta C in float32 on tcgen05: A m x k and B n x k row-major (k
 // contiguous), lda, ldb % 4 == 0, 16-byte bases; C row-major, and when ct is not NULL its
 // transpose goes to ct (ldct) too. passes 1: TF32 inputs; passes 3: float32-level products.
+// max_ctas > 0 caps the persistent grid (to leave SMs to a kernel on another stream).
 int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* b,
              int64_t ldb, float beta, float* c, int64_t ldc, unsigned* status, cudaStream_t stream,
-             float* ct = nullptr, int64_t ldct = 0);
+             float* ct = nullptr, int64_t ldct = 0, int max_ctas = 0);
 int transpose_f32(const float* src, int64_t lds, int64_t m, int64_t n, float* dst, int64_t ldd, cudaStream_t stream);
 int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStream_t stream);
 int split_lo_f32(const float* x, int64_t ldx, int64_t m, int64_t k, float* lo, int64_t ldl, cudaStream_t stream);

@@ -390,7 +390,7 @@ int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStrea
 template <int PASSES, bool TMA_EPI>
 static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tcm, float* c, int64_t ldc,
                         float* ct, int64_t ldct, int m, int n, int k, float alpha, float beta, unsigned* status,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int max_ctas) {
   using C = tc::Cfg<PASSES>;
   static bool set = false;
   if (!set) {
@@ -399,7 +399,8 @@ static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, const CUte
     set = true;
   }
   const int64_t tiles = (int64_t)((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN);
-  const unsigned grid = (unsigned)std::min<int64_t>(tiles, device_sm_count());
+  const int ctas = max_ctas > 0 ? std::min(max_ctas, device_sm_count()) : device_sm_count();
+  const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctas);
   sgemm_tc_kernel<PASSES, TMA_EPI><<<grid, C::THREADS, C::SMEM, stream>>>(ta, tb, tcm, c, ldc, ct, ldct, m, n, k,
                                                                           alpha, beta, status);
   RM_LAUNCHED();
@@ -408,7 +409,7 @@ static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, const CUte
 
 int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* b,
              int64_t ldb, float beta, float* c, int64_t ldc, unsigned* status, cudaStream_t stream, float* ct,
-             int64_t ldct) {
+             int64_t ldct, int max_ctas) {
   if (m == 0 || n == 0) return RM_OK;
   if (passes != 1 && passes != 3) return RM_BAD_ARG;
   if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || k == 0) return RM_BAD_ARG;
@@ -423,10 +424,10 @@ int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const flo
   else memset(&tcm, 0, sizeof tcm);
   const int mi = (int)m, ni = (int)n, ki = (int)k;
   if (passes == 3)
-    return tma_epi ? launch_sgemm<3, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream)
-                   : launch_sgemm<3, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream);
-  return tma_epi ? launch_sgemm<1, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream)
-                 : launch_sgemm<1, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream);
+    return tma_epi ? launch_sgemm<3, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas)
+                   : launch_sgemm<3, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas);
+  return tma_epi ? launch_sgemm<1, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas)
+                 : launch_sgemm<1, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas);
 }
 
 // dst (n x m, ldd) = src^T for the m x n row-major float32 src (lds): 32x32 tiles through

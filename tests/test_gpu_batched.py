@@ -159,3 +159,24 @@ def test_device_lists(rb):
     Xs, rep = rb.solve_batched(ta, tb)
     assert Xs[1].shape == (130,) and Xs[1].is_cuda
     check_bar(As, Bs, [Xs[0].cpu().numpy(), Xs[1].cpu().numpy().reshape(-1, 1)])
+
+
+def test_host_form(rb):
+    import ctypes
+    from rustymath_b200 import _lib
+    sizes, ks = [12, 100, 3], [2, 1, 4]
+    As, Bs = batch(sizes, ks, general, seed=40)
+    plan_ns, plan_ks = np.array(sizes, np.int64), np.array(ks, np.int64)
+    a_off = np.array([0, 144, 144 + 10000], np.int64)
+    b_off = np.array([0, 24, 124], np.int64)
+    a = np.concatenate([x.ravel() for x in As])
+    b = np.concatenate([x.ravel() for x in Bs])
+    x = np.zeros_like(b)
+    rep = _lib.BatchReport()
+    opts = rb.linalg._options("mixed")
+    st = _lib.load().rm_dsolve_batched_host(3, plan_ns.ctypes.data, plan_ks.ctypes.data, a_off.ctypes.data,
+                                            b_off.ctypes.data, b_off.ctypes.data, a.ctypes.data, b.ctypes.data,
+                                            x.ctypes.data, ctypes.byref(opts), ctypes.byref(rep))
+    _lib.check(st, "rm_dsolve_batched_host")
+    Xs = [x[o:o + n * k].reshape(n, k) for o, n, k in zip(b_off, sizes, ks)]
+    check_bar(As, Bs, Xs)

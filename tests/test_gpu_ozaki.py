@@ -65,3 +65,13 @@ def test_zero_rows_columns_and_k_zero():
     assert np.allclose(got, a @ b, rtol=1e-13, atol=1e-13 * np.abs(a @ b).max())
     z = run(np.zeros((5, 0)), np.zeros((0, 4)), 8)
     assert (z == 0).all() and z.shape == (5, 4)
+
+
+def test_host_form():
+    from rustymath_b200 import _lib
+    a, b = wide(130, 77, 60, 3)
+    c = np.zeros((130, 60))
+    st = _lib.load().rm_dgemm_ozaki_host(130, 60, 77, a.ctypes.data, 77, b.ctypes.data, 60, c.ctypes.data, 60, 8)
+    _lib.check(st, "rm_dgemm_ozaki_host")
+    ref = exact(a, b)
+    assert (np.abs(c.astype(np.longdouble) - ref).astype(np.float64) <= 4 * 2.0 ** -53 * 7 * (np.abs(a) @ np.abs(b))).all()

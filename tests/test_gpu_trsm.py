@@ -43,3 +43,16 @@ def test_trsm_matches_lapack(side, uplo, trans, diag, m, n):
 def test_trsm_bad_codes():
     from rustymath_b200 import _lib
     assert _lib.load().rm_dtrsm(140, 121, 111, 131, 2, 2, None, 2, None, 2, None) == _lib.RM_BAD_ARG
+
+
+def test_trsm_host_form():
+    from rustymath_b200 import _lib
+    rng = np.random.default_rng(9)
+    m, n = 90, 7
+    a = np.tril(rng.standard_normal((n, n))) + 3 * np.eye(n)
+    x = rng.standard_normal((m, n))
+    want = np.linalg.solve(a.T, x.T).T  # x a^-1: side right, lower, no transpose, non-unit
+    got = x.copy()
+    st = _lib.load().rm_dtrsm_host(142, 122, 111, 131, m, n, a.ctypes.data, n, got.ctypes.data, n)
+    _lib.check(st, "rm_dtrsm_host")
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-12)
