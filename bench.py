@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--solve-only", action="store_true",
                    help="only the timed solves (for profiling): no e2e, roofline or CPU legs")
-    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm", "update"],
+    p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm", "update", "small"],
                    help="single: the n=8192 system (the headline); batched: 20,000 uneven systems")
     p.add_argument("--count", type=int, default=20000, help="systems in the batched workload")
     return p.parse_args()
@@ -483,6 +483,79 @@ def run_gemm(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_small(args, rank, world, local):
+    """The size rustymath already runs on CPU: one n = 512 system (A = N(0,1) + 512 I, b ~ N(0,1),
+    nrhs = 1) by the plain and the mixed method, and C = A B at 512^3 (U(-1,1)); against the
+    oracle on 1 host thread and on all of them. Device time per call (CUDA events) and the
+    host-pointer call's wall time."""
+    import torch
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(dev)
+    import rustymath_b200 as rb
+    from rustymath_b200 import _lib
+    from oracle import oracle as O
+    lib = _lib.load()
+    n = 512
+    rng = np.random.default_rng(0)
+    a_h = rng.standard_normal((n, n)) + n * np.eye(n)
+    b_h = rng.standard_normal((n, 1))
+    ga, gb = rng.uniform(-1, 1, (n, n)), rng.uniform(-1, 1, (n, n))
+    a, b = torch.tensor(a_h, device=dev), torch.tensor(b_h, device=dev)
+    x = torch.empty_like(b)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    reps = max(args.steps, 20)
+
+    def dev_time(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    def host_time(fn):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps
+
+    out = {}
+    for meth in ("plain", "mixed"):
+        opts = rb.linalg._options(meth)
+        rep = _lib.SolveReport()
+        xs = np.zeros((n, 1))
+        out[f"solve_{meth}_ms"] = 1e3 * dev_time(lambda: lib.rm_dsolve(n, a.data_ptr(), b.data_ptr(), 1, x.data_ptr(),
+                                                                         ctypes.byref(opts), ctypes.byref(rep), sp))
+        out[f"solve_{meth}_host_ms"] = 1e3 * host_time(lambda: lib.rm_dsolve_host(
+            n, a_h.ctypes.data, b_h.ctypes.data, 1, xs.ctypes.data, ctypes.byref(opts), ctypes.byref(rep)))
+        out[f"solve_{meth}_backward_error"] = O.backward_error(a_h, xs, b_h)
+        xo = O.solve(a_h, b_h)
+        out[f"solve_{meth}_max_rel_diff_vs_oracle"] = float(np.abs(xs - xo).max() / np.abs(xo).max())
+    ta, tb = torch.tensor(ga, device=dev), torch.tensor(gb, device=dev)
+    tc = torch.empty_like(ta)
+    out["matmul_ms"] = 1e3 * dev_time(lambda: lib.rm_dgemm(0, 0, n, n, n, 1.0, ta.data_ptr(), n, tb.data_ptr(), n, 0.0,
+                                                             tc.data_ptr(), n, sp))
+    cref = O.dgemm(ga, gb)
+    out["matmul_max_abs_diff_vs_oracle"] = float(np.abs(tc.cpu().numpy() - cref).max())
+    cpu = {}
+    for threads in (1, os.cpu_count()):
+        O.set_threads(threads)
+        cpu[f"solve_ms_{threads}t"] = 1e3 * host_time(lambda: O.solve(a_h, b_h))
+        cpu[f"matmul_ms_{threads}t"] = 1e3 * host_time(lambda: O.dgemm(ga, gb))
+    line = {"metric": "n=512 solve and 512^3 matmul (the size rustymath runs on CPU)", "value": 1e3 / out["solve_plain_ms"],
+            "unit": "solves/s (plain, device time)", "n_gpus": world, "steps": reps, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": "n=512 nrhs=1, A=N(0,1)+512 I; 512^3 U(-1,1)"},
+            "gpu": out, "cpu_baseline": {"kind": "port", "cores": os.cpu_count(), **cpu},
+            "gflops": {"solve_plain": (2 / 3 * n ** 3 + 2 * n * n) / out["solve_plain_ms"] / 1e6,
+                       "matmul": 2 * n ** 3 / out["matmul_ms"] / 1e6}}
+    print(json.dumps(line), flush=True)
+
+
 def run_update(args, rank, world, local):
     """The headline roofline's kernel alone: the mixed LU's first rank-128 trailing update
     (3xTF32 tcgen05, m = n = n - 128, k = 128, beta = 1), timed by CUDA events (for profiling)."""
@@ -512,6 +585,8 @@ def main():
         return run_gemm(args, rank, world, local)
     if args.workload == "update":
         return run_update(args, rank, world, local)
+    if args.workload == "small":
+        return run_small(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
