@@ -17,7 +17,7 @@
 //     never chosen over a number); then U12 of the panel's pivot rows (a column per thread)
 //     and the update of the rows not chosen yet;
 //   - solves L U x = P b with the rows' right-hand sides in registers, block by block (a warp
-//     solves each NB x NB diagonal block with shuffles);
+//     per right-hand side solves each NB x NB diagonal block with shuffles);
 //   - refines in float64: r = b - A x (a warp per row of A, x in shared memory), the normwise
 //     backward error max_c ||r_c|| / (||A|| ||x_c|| + ||b_c||), and corrections from the
 //     float32 factors until it is at most the tolerance (n * 2^-53 by default);
@@ -51,9 +51,9 @@ struct Smem {
   alignas(16) unsigned char slot[2][WARPS][SLOT_BYTES];  // posts: NB items, then key (T), row
   alignas(16) unsigned char lp[32 * 36 * 4];              // the panel's pivot rows (NB x (NB + 4) items)
   alignas(16) unsigned char ubt[UBT_BYTES];               // U12 of a panel, transposed
-  alignas(16) double xs[NMAX][KMAX];                      // the float64 solution, by unknown
-  alignas(16) double rs[NMAX][KMAX];                      // the float64 residual, by row
-  alignas(16) double vsm[32][KMAX];                       // a diagonal block's right-hand sides
+  alignas(16) double xs[NMAX][KMAX + 1];                  // the float64 solution, by unknown (rows
+  alignas(16) double rs[NMAX][KMAX + 1];                  //  padded: a warp's rows on distinct banks)
+  alignas(16) double vsm[32][KMAX + 1];                   // a diagonal block's right-hand sides
   int piv[NMAX];                                          // logical position -> row
   double red[WARPS][3 * KMAX + 1];
   double anorm, bnorm[KMAX];
@@ -220,26 +220,21 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
 #pragma unroll
       for (int c = 0; c < KMAX; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
     __syncthreads();
-    if (warp == 0) {
-      T y[KMAX], lrow[NB];
+    if (warp < k) {  // a warp per right-hand side: column c = warp, lane = row of the block
+      const int c = warp;
+      T lrow[NB];
       const T* prow = W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J;
-#pragma unroll
-      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+      T y = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q) lrow[q] = (lane < nbj && q < lane) ? prow[q] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q) {
         if (q < nbj) {
-#pragma unroll
-          for (int c = 0; c < KMAX; ++c) {
-            const T yq = __shfl_sync(0xffffffffu, y[c], q);
-            if (lane > q) y[c] = fma(-lrow[q], yq, y[c]);
-          }
+          const T yq = __shfl_sync(0xffffffffu, y, q);
+          if (lane > q) y = fma(-lrow[q], yq, y);
         }
       }
-      if (lane < nbj)
-#pragma unroll
-        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+      if (lane < nbj) sm.vsm[lane][c] = (double)y;
     }
     __syncthreads();
     if (r < n) {
@@ -249,7 +244,8 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
           if (q < nbj) {
             const T l = row[J + q];
 #pragma unroll
-            for (int c = 0; c < KMAX; ++c) v[c] = fma(-l, (T)sm.vsm[q][c], v[c]);
+            for (int c = 0; c < KMAX; ++c)
+              if (c < k) v[c] = fma(-l, (T)sm.vsm[q][c], v[c]);
           }
       } else if (my_pos >= J) {
 #pragma unroll
@@ -266,27 +262,22 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
 #pragma unroll
       for (int c = 0; c < KMAX; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
     __syncthreads();
-    if (warp == 0) {
-      T y[KMAX], urow[NB];
+    if (warp < k) {  // a warp per right-hand side
+      const int c = warp;
+      T urow[NB];
       const T* prow = W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J;
-#pragma unroll
-      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+      T y = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q) urow[q] = (lane < nbj && q >= lane && q < nbj) ? prow[q] : T(0);
 #pragma unroll
       for (int q = NB - 1; q >= 0; --q) {
         if (q < nbj) {
-#pragma unroll
-          for (int c = 0; c < KMAX; ++c) {
-            if (lane == q) y[c] = y[c] / urow[q];
-            const T xq = __shfl_sync(0xffffffffu, y[c], q);
-            if (lane < q) y[c] = fma(-urow[q], xq, y[c]);
-          }
+          if (lane == q) y = y / urow[q];
+          const T xq = __shfl_sync(0xffffffffu, y, q);
+          if (lane < q) y = fma(-urow[q], xq, y);
         }
       }
-      if (lane < nbj)
-#pragma unroll
-        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+      if (lane < nbj) sm.vsm[lane][c] = (double)y;
     }
     __syncthreads();
     if (r < n) {
@@ -296,7 +287,8 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
           if (q < nbj) {
             const T u = row[J + q];
 #pragma unroll
-            for (int c = 0; c < KMAX; ++c) v[c] = fma(-u, (T)sm.vsm[q][c], v[c]);
+            for (int c = 0; c < KMAX; ++c)
+              if (c < k) v[c] = fma(-u, (T)sm.vsm[q][c], v[c]);
           }
       } else if (my_pos >= J && my_pos < J + nbj) {
 #pragma unroll
@@ -328,13 +320,15 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
       const double av = __ldg(ar + j);
       asum += fabs(av);
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c) acc[c] = fma(av, sm.xs[j][c], acc[c]);
+      for (int c = 0; c < KMAX; ++c)
+        if (c < k) acc[c] = fma(av, sm.xs[j][c], acc[c]);
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
       asum += __shfl_xor_sync(0xffffffffu, asum, off);
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+      for (int c = 0; c < KMAX; ++c)
+        if (c < k) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
     }
     amax = fmax(amax, asum);
     if (lane < k) {
@@ -554,29 +548,22 @@ __device__ void bsolve_t(const T* W, int ld, int n, int k, Smem& sm, T (&v)[KMAX
 #pragma unroll
       for (int c = 0; c < KMAX; ++c) sm.vsm[t - J][c] = (double)v[c];
     __syncthreads();
-    if (warp == 0) {
-      T y[KMAX], ucol[NB];
-#pragma unroll
-      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+    if (warp < k) {  // a warp per right-hand side
+      const int c = warp;
+      T ucol[NB];
+      T y = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q)  // U[J+q][J+lane], q <= lane
         ucol[q] = (lane < nbj && q <= lane) ? W[(int64_t)sm.piv[J + q] * ld + J + lane] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q) {
         if (q < nbj) {
-#pragma unroll
-          for (int c = 0; c < KMAX; ++c) {
-            if (c < k) {
-              if (lane == q) y[c] = y[c] / ucol[q];
-              const T zq = __shfl_sync(0xffffffffu, y[c], q);
-              if (lane > q) y[c] = fma(-ucol[q], zq, y[c]);
-            }
-          }
+          if (lane == q) y = y / ucol[q];
+          const T zq = __shfl_sync(0xffffffffu, y, q);
+          if (lane > q) y = fma(-ucol[q], zq, y);
         }
       }
-      if (lane < nbj)
-#pragma unroll
-        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+      if (lane < nbj) sm.vsm[lane][c] = (double)y;
     }
     __syncthreads();
     if (t < n) {
@@ -601,28 +588,21 @@ __device__ void bsolve_t(const T* W, int ld, int n, int k, Smem& sm, T (&v)[KMAX
 #pragma unroll
       for (int c = 0; c < KMAX; ++c) sm.vsm[t - J][c] = (double)v[c];
     __syncthreads();
-    if (warp == 0) {
-      T y[KMAX], lcol[NB];
-#pragma unroll
-      for (int c = 0; c < KMAX; ++c) y[c] = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
+    if (warp < k) {  // a warp per right-hand side
+      const int c = warp;
+      T lcol[NB];
+      T y = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q)  // L[J+q][J+lane], q > lane
         lcol[q] = (lane < nbj && q > lane && q < nbj) ? W[(int64_t)sm.piv[J + q] * ld + J + lane] : T(0);
 #pragma unroll
       for (int q = NB - 1; q >= 0; --q) {
         if (q < nbj) {
-#pragma unroll
-          for (int c = 0; c < KMAX; ++c) {
-            if (c < k) {
-              const T wq = __shfl_sync(0xffffffffu, y[c], q);
-              if (lane < q) y[c] = fma(-lcol[q], wq, y[c]);
-            }
-          }
+          const T wq = __shfl_sync(0xffffffffu, y, q);
+          if (lane < q) y = fma(-lcol[q], wq, y);
         }
       }
-      if (lane < nbj)
-#pragma unroll
-        for (int c = 0; c < KMAX; ++c) sm.vsm[lane][c] = (double)y[c];
+      if (lane < nbj) sm.vsm[lane][c] = (double)y;
     }
     __syncthreads();
     if (t < n) {
