@@ -36,7 +36,8 @@ namespace rm {
 constexpr int kLppCols = 128;  // panel width (the trailing update's rank)
 constexpr int kLppRows = 256;  // rows a panel's pivots are chosen among
 constexpr int kLppLeaf = 32;
-constexpr int kLppThreads = 256;
+constexpr int kLppThreads = 256;  // a thread per row
+constexpr int kLppPRows = 2 * kLppCols;  // rows of the panel buffer (the inverses use its upper half)
 constexpr int kLppStride = kLppCols + 1;
 
 __device__ __forceinline__ void warp_argmax_f32(float& v, int& i) {
@@ -64,21 +65,17 @@ __global__ void to_f32_kernel(const double* __restrict__ a, int64_t lda, int64_t
 // ------------------------------------------------------------------ the panel
 struct alignas(16) LppSlot {
   float row[kLppLeaf];  // a warp's candidate pivot row (its current leaf columns)
-  float key;            // its |pivot|; -0.5 for NaN, -1 when the warp has no candidate
-  int idx;
-  int pad[2];
+  unsigned key;         // its |pivot| as an ordered key: bits + 2; 1 for NaN; 0: no candidate
+  int idx;              // its row
+  float rcp;            // 1 / pivot
+  int pad;
 };
 
-__device__ __forceinline__ void warp_argmax_key(float& v, int& i) {
-#pragma unroll
-  for (int off = 16; off; off >>= 1) {
-    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
-    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
-    if (ov > v || (ov == v && oi < i)) {
-      v = ov;
-      i = oi;
-    }
-  }
+// |v| as an unsigned key ordered like the magnitudes: 0 is no candidate, 1 a NaN (never chosen
+// over a number), otherwise the float's bits + 2 (non-negative floats order like their bits).
+__device__ __forceinline__ unsigned pivot_key(float v) {
+  const float a = fabsf(v);
+  return a != a ? 1u : __float_as_uint(a) + 2u;
 }
 
 // Factors the T x nb panel A[j0.., j0..] (T <= 256, nb <= 128) with partial pivoting among
@@ -100,8 +97,8 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
                                                                 unsigned* status) {
   extern __shared__ float sm[];
   float(*P)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm);
-  float(*X)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm + kLppRows * kLppStride);
-  float(*Tm)[33] = reinterpret_cast<float(*)[33]>(sm + (kLppRows + kLppCols) * kLppStride);  // 96 x 33
+  float(*X)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm + kLppPRows * kLppStride);
+  float(*Tm)[33] = reinterpret_cast<float(*)[33]>(sm + (kLppPRows + kLppCols) * kLppStride);  // 96 x 33
   // during the factorization X's space holds the leaf's U12, transposed (column j's 32 values contiguous)
   float(*UbT)[kLppLeaf + 4] = reinterpret_cast<float(*)[kLppLeaf + 4]>(X);
   __shared__ LppSlot slot[2][kLppThreads / 32];
@@ -129,33 +126,26 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
     for (int c = 0; c < kLppLeaf; ++c) {
       if (c0 + c >= nb) continue;  // the last panel may be narrower than a leaf
       LppSlot* sl = &slot[c & 1][0];
-      float key = -1.0f;
-      if (active) {
-        const float v = fabsf(p[c]);
-        key = v != v ? -0.5f : v;
-      }
-      int idx = r;
-      warp_argmax_key(key, idx);
-      if (lane == (idx & 31)) {  // the warp's candidate (any lane when the warp has none)
+      // the warp's candidate: the largest key (redux), the lowest lane holding it (ballot)
+      const unsigned key = active ? pivot_key(p[c]) : 0u;
+      const unsigned wmax = __reduce_max_sync(0xffffffffu, key);
+      const int wl = __ffs(__ballot_sync(0xffffffffu, key == wmax)) - 1;
+      if (lane == wl) {
         float4* dst = reinterpret_cast<float4*>(sl[warp].row);
 #pragma unroll
         for (int i = 0; i < kLppLeaf / 4; ++i) dst[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
-        sl[warp].key = key;
-        sl[warp].idx = idx;
+        sl[warp].key = wmax;
+        sl[warp].idx = r;
+        sl[warp].rcp = __frcp_rn(p[c]);
       }
       __syncthreads();
-      float bk = sl[0].key;
-      int bi = sl[0].idx, bw = 0;
-#pragma unroll
-      for (int w = 1; w < kLppThreads / 32; ++w) {
-        const float k2 = sl[w].key;
-        const int i2 = sl[w].idx;
-        if (k2 > bk || (k2 == bk && i2 < bi)) {
-          bk = k2;
-          bi = i2;
-          bw = w;
-        }
-      }
+      // the winning post: the largest key, the lowest warp (so the lowest row) among equals
+      const unsigned kq = lane < kLppThreads / 32 ? sl[lane].key : 0u;
+      const unsigned gmax = __reduce_max_sync(0xffffffffu, kq);
+      const unsigned gball = __ballot_sync(0xffffffffu, lane < kLppThreads / 32 && kq == gmax);
+      const int bw = gball ? __ffs(gball) - 1 : 0;
+      const int bi = sl[bw].idx;
+      const float prcp = sl[bw].rcp;
       // the pivot row, as 16-byte reads of the winning post
       float prow[kLppLeaf];
       {
@@ -177,7 +167,7 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
         }
       }
       if (active && piv != 0.0f) {
-        const float l = p[c] * __frcp_rn(piv);
+        const float l = p[c] * prcp;
         p[c] = l;
 #pragma unroll
         for (int i = c + 1; i < kLppLeaf; ++i) p[i] = fmaf(-l, prow[i], p[i]);
@@ -212,17 +202,17 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
     // the rows still unchosen: later columns -= L(row, leaf) U12
     if (active) {
       for (int j = 0; j < rcols; ++j) {
-        float acc = P[r][rc0 + j];
+        float a0 = P[r][rc0 + j], a1 = 0.f, a2 = 0.f, a3 = 0.f;  // four chains
         const float4* ub = reinterpret_cast<const float4*>(&UbT[j][0]);
 #pragma unroll
         for (int q = 0; q < kLppLeaf / 4; ++q) {
           const float4 u4 = ub[q];
-          acc = fmaf(-p[4 * q], u4.x, acc);
-          acc = fmaf(-p[4 * q + 1], u4.y, acc);
-          acc = fmaf(-p[4 * q + 2], u4.z, acc);
-          acc = fmaf(-p[4 * q + 3], u4.w, acc);
+          a0 = fmaf(-p[4 * q], u4.x, a0);
+          a1 = fmaf(-p[4 * q + 1], u4.y, a1);
+          a2 = fmaf(-p[4 * q + 2], u4.z, a2);
+          a3 = fmaf(-p[4 * q + 3], u4.w, a3);
         }
-        P[r][rc0 + j] = acc;
+        P[r][rc0 + j] = (a0 + a1) + (a2 + a3);
       }
     }
     __syncthreads();
@@ -265,72 +255,77 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
   for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32)
     for (int c = lane; c < kLppCols; c += 32) D[rr][c] = X[rr][c];
   __syncthreads();
-  if (warp < 4) {
-    const int b0 = warp * 32;
+  for (int job = warp; job < 8; job += kLppThreads / 32) {  // 4 blocks of L11, then 4 of U11^T
+    const int b0 = (job & 3) * 32;
     float x[32];
+    if (job < 4) {
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      float acc = i == lane ? 1.0f : 0.0f;
+      for (int i = 0; i < 32; ++i) {
+        float acc = i == lane ? 1.0f : 0.0f;
 #pragma unroll
-      for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + i][b0 + k2], x[k2], acc);
-      x[i] = i < lane ? 0.0f : acc;
+        for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + i][b0 + k2], x[k2], acc);
+        x[i] = i < lane ? 0.0f : acc;
+      }
+#pragma unroll
+      for (int i = 0; i < 32; ++i) XL[b0 + i][b0 + lane] = x[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        float acc = i == lane ? 1.0f : 0.0f;
+#pragma unroll
+        for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + k2][b0 + i], x[k2], acc);
+        x[i] = i < lane ? 0.0f : acc / D[b0 + i][b0 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 32; ++i) XU[b0 + i][b0 + lane] = x[i];
     }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) XL[b0 + i][b0 + lane] = x[i];
-  } else {
-    const int b0 = (warp - 4) * 32;
-    float x[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      float acc = i == lane ? 1.0f : 0.0f;
-#pragma unroll
-      for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + k2][b0 + i], x[k2], acc);
-      x[i] = i < lane ? 0.0f : acc / D[b0 + i][b0 + i];
-    }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) XU[b0 + i][b0 + lane] = x[i];
   }
   __syncthreads();
   {
-    const int ti = tid >> 4, tj = tid & 15;  // rows ti, ti+16 and columns tj, tj+16 of a block
-    float(*Tq)[33] = Tm;                     // up to 3 blocks of 32 x 33
+    float(*Tq)[33] = Tm;  // up to 3 blocks of 32 x 33
     for (int gap = 1; gap < 4; ++gap)
       for (int m = 0; m < 2; ++m) {
         float(*Xm)[kLppStride] = m == 0 ? XL : XU;
         for (int a = 0; a + gap < 4; ++a) {
           const int b = a + gap;
-          float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
-          const int r0 = 32 * b + ti, r1 = r0 + 16, c0 = 32 * a + tj, c1 = c0 + 16;
-          if (m == 0) {
+          for (int tp = tid; tp < 256; tp += kLppThreads) {  // rows ti, ti+16, columns tj, tj+16
+            const int ti = tp >> 4, tj = tp & 15;
+            float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
+            const int r0 = 32 * b + ti, r1 = r0 + 16, c0 = 32 * a + tj, c1 = c0 + 16;
+            if (m == 0) {
 #pragma unroll 4
-            for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
-              const float m0 = D[r0][k2], m1 = D[r1][k2], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
-              t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
-            }
-          } else {
+              for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
+                const float m0 = D[r0][k2], m1 = D[r1][k2], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
+                t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
+              }
+            } else {
 #pragma unroll 4
-            for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
-              const float m0 = D[k2][r0], m1 = D[k2][r1], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
-              t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
+              for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
+                const float m0 = D[k2][r0], m1 = D[k2][r1], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
+                t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
+              }
             }
+            float(*T1)[33] = Tq + 32 * a;
+            T1[ti][tj] = t00, T1[ti][tj + 16] = t01, T1[ti + 16][tj] = t10, T1[ti + 16][tj + 16] = t11;
           }
-          float(*T1)[33] = Tq + 32 * a;
-          T1[ti][tj] = t00, T1[ti][tj + 16] = t01, T1[ti + 16][tj] = t10, T1[ti + 16][tj + 16] = t11;
         }
         __syncthreads();
         for (int a = 0; a + gap < 4; ++a) {
           const int b = a + gap;
           float(*T1)[33] = Tq + 32 * a;
-          float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
-          const int r0 = 32 * b + ti, r1 = r0 + 16;
+          for (int tp = tid; tp < 256; tp += kLppThreads) {
+            const int ti = tp >> 4, tj = tp & 15;
+            float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
+            const int r0 = 32 * b + ti, r1 = r0 + 16;
 #pragma unroll 4
-          for (int k2 = 0; k2 < 32; ++k2) {
-            const float x0 = Xm[r0][32 * b + k2], x1 = Xm[r1][32 * b + k2];
-            const float u0 = T1[k2][tj], u1 = T1[k2][tj + 16];
-            t00 = fmaf(x0, u0, t00), t01 = fmaf(x0, u1, t01), t10 = fmaf(x1, u0, t10), t11 = fmaf(x1, u1, t11);
+            for (int k2 = 0; k2 < 32; ++k2) {
+              const float x0 = Xm[r0][32 * b + k2], x1 = Xm[r1][32 * b + k2];
+              const float u0 = T1[k2][tj], u1 = T1[k2][tj + 16];
+              t00 = fmaf(x0, u0, t00), t01 = fmaf(x0, u1, t01), t10 = fmaf(x1, u0, t10), t11 = fmaf(x1, u1, t11);
+            }
+            Xm[r0][32 * a + tj] = -t00, Xm[r0][32 * a + tj + 16] = -t01, Xm[r1][32 * a + tj] = -t10,
+                            Xm[r1][32 * a + tj + 16] = -t11;
           }
-          Xm[r0][32 * a + tj] = -t00, Xm[r0][32 * a + tj + 16] = -t01, Xm[r1][32 * a + tj] = -t10,
-                          Xm[r1][32 * a + tj + 16] = -t11;
         }
         __syncthreads();
       }
@@ -342,7 +337,7 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
     }
 }
 
-constexpr size_t kLppSmem = ((size_t)(kLppRows + kLppCols) * kLppStride + 3 * 32 * 33) * sizeof(float);
+constexpr size_t kLppSmem = ((size_t)(kLppPRows + kLppCols) * kLppStride + 3 * 32 * 33) * sizeof(float);
 
 // ------------------------------------------------------------------ the panel's row permutation
 constexpr int kApplyCols = 32;
