@@ -119,30 +119,51 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
       if (c < nbj) {
         unsigned char(*sl)[SLOT_BYTES] = sm.slot[c & 1];
         T key = T(-1);
-        if (active) {
-          const T v = tabs(p[c]);
-          key = v != v ? T(-0.5) : v;
-        }
-        int idx = r;
-        warp_argmax(key, idx);
-        if (lane == (idx & 31)) {
-          T* post = reinterpret_cast<T*>(sl[warp]);
+        int idx = r, bi, bw;
+        if (sizeof(T) == 4) {
+          // float: |pivot| as an ordered 32-bit key (0 none, 1 NaN, bits + 2), redux max + ballot
+          const float v = fabsf((float)p[c]);
+          const unsigned uk = active ? (v != v ? 1u : __float_as_uint(v) + 2u) : 0u;
+          const unsigned wmax = __reduce_max_sync(0xffffffffu, uk);
+          const int wl = __ffs(__ballot_sync(0xffffffffu, uk == wmax)) - 1;
+          if (lane == wl) {
+            T* post = reinterpret_cast<T*>(sl[warp]);
 #pragma unroll
-          for (int i = 0; i < NB; ++i) post[i] = p[i];
-          *reinterpret_cast<T*>(sl[warp] + 128) = key;
-          *reinterpret_cast<int*>(sl[warp] + 136) = idx;
-        }
-        __syncthreads();
-        T bk = *reinterpret_cast<const T*>(sl[0] + 128);
-        int bi = *reinterpret_cast<const int*>(sl[0] + 136), bw = 0;
+            for (int i = 0; i < NB; ++i) post[i] = p[i];
+            *reinterpret_cast<unsigned*>(sl[warp] + 128) = wmax;
+            *reinterpret_cast<int*>(sl[warp] + 136) = r;
+          }
+          __syncthreads();
+          const unsigned kq = lane < WARPS ? *reinterpret_cast<const unsigned*>(sl[lane] + 128) : 0u;
+          const unsigned gmax = __reduce_max_sync(0xffffffffu, kq);
+          const unsigned gball = __ballot_sync(0xffffffffu, lane < WARPS && kq == gmax);
+          bw = gball ? __ffs(gball) - 1 : 0;
+          bi = *reinterpret_cast<const int*>(sl[bw] + 136);
+        } else {
+          if (active) {
+            const T v = tabs(p[c]);
+            key = v != v ? T(-0.5) : v;
+          }
+          warp_argmax(key, idx);
+          if (lane == (idx & 31)) {
+            T* post = reinterpret_cast<T*>(sl[warp]);
 #pragma unroll
-        for (int w = 1; w < WARPS; ++w) {
-          const T k2 = *reinterpret_cast<const T*>(sl[w] + 128);
-          const int i2 = *reinterpret_cast<const int*>(sl[w] + 136);
-          if (k2 > bk || (k2 == bk && i2 < bi)) {
-            bk = k2;
-            bi = i2;
-            bw = w;
+            for (int i = 0; i < NB; ++i) post[i] = p[i];
+            *reinterpret_cast<T*>(sl[warp] + 128) = key;
+            *reinterpret_cast<int*>(sl[warp] + 136) = idx;
+          }
+          __syncthreads();
+          T bk = *reinterpret_cast<const T*>(sl[0] + 128);
+          bi = *reinterpret_cast<const int*>(sl[0] + 136), bw = 0;
+#pragma unroll
+          for (int w = 1; w < WARPS; ++w) {
+            const T k2 = *reinterpret_cast<const T*>(sl[w] + 128);
+            const int i2 = *reinterpret_cast<const int*>(sl[w] + 136);
+            if (k2 > bk || (k2 == bk && i2 < bi)) {
+              bk = k2;
+              bi = i2;
+              bw = w;
+            }
           }
         }
         const T* prow = reinterpret_cast<const T*>(sl[bw]);
