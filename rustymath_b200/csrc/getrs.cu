@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(TB * 4)
   extern __shared__ uint8_t smraw[];
   T(*lblk)[LDS] = reinterpret_cast<T(*)[LDS]>(smraw);
   T(*xs)[kKC] = reinterpret_cast<T(*)[kKC]>(smraw + ((size_t)TB * LDS * sizeof(T) + 15) / 16 * 16);
-  __shared__ int ticket, good;
+  __shared__ int ticket;
   const int tid = threadIdx.x;
   const int nblk = (n + TB - 1) / TB;
   if (tid == 0) ticket = atomicAdd(counter, 1);
@@ -257,26 +257,28 @@ __global__ void __launch_bounds__(TB * 4)
     }
   };
   // waits (bounded) for block j's release, then stages x_j in xs
+  // waits (bounded) for block j's release and stages x_j in xs: every thread acquires the flag
+  // itself and loads its share at once, and one barrier (which also agrees on the outcome)
+  // closes the step
   auto fetch = [&](int j) -> bool {
-    if (tid == 0) {
-      bool seen = ld_acquire(&flags[j]) != 0;
-      if (!seen) {
-        const uint64_t start = global_ns();
-        while (!(seen = ld_acquire(&flags[j]) != 0)) {
-          if (global_ns() - start > kWaitLimitNs) break;
-        }
+    bool seen = ld_acquire(&flags[j]) != 0;
+    if (!seen) {
+      const uint64_t start = global_ns();
+      while (!(seen = ld_acquire(&flags[j]) != 0)) {
+        if (global_ns() - start > kWaitLimitNs) break;
       }
-      if (!seen) flag_error(status, RM_DEV_TIMEOUT);
-      good = seen ? 1 : 0;
     }
-    __syncthreads();
-    if (!good) return false;
-    const int c0 = j * TB, cols = min(TB, n - c0);
-    for (int e = tid; e < TB * kKC; e += THREADS) {
-      const int r = e / kKC, c = e % kKC;
-      xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : T(0);
+    if (seen) {
+      const int c0 = j * TB, cols = min(TB, n - c0);
+      for (int e = tid; e < TB * kKC; e += THREADS) {
+        const int r = e / kKC, c = e % kKC;
+        xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : T(0);
+      }
     }
-    __syncthreads();
+    if (!__syncthreads_and(seen ? 1 : 0)) {
+      if (tid == 0) flag_error(status, RM_DEV_TIMEOUT);
+      return false;
+    }
     return true;
   };
 
@@ -348,12 +350,10 @@ __global__ void __launch_bounds__(TB * 4)
     }
   }
   }
-  // every thread's x is written before the barrier; one fence makes them visible device-wide
+  // every thread's x is written before the barrier; thread 0's release store, ordered after the
+  // barrier, publishes them device-wide
   __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    st_release(&flags[b], 1);
-  }
+  if (tid == 0) st_release(&flags[b], 1);
 }
 
 template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE = false>
