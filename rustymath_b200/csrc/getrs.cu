@@ -186,32 +186,66 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // between seeing p's flag and releasing its own. Thread t owns row t / 4 and columns
 // 4 (t % 4) .. +3 of its block's sums. The next matrix a step needs is loaded into registers
 // while the current one is applied, so each block of T crosses HBM once.
+// Shared-memory layout of a chain CTA. float32 with 128-row blocks multiplies on the tensor
+// cores (mma.sync m16n8k8, TF32 inputs split into high and low parts, three products: float32-
+// level accuracy); the padded rows keep its fragment loads free of bank conflicts.
+template <typename T, int TB>
+struct ChainLayout {
+  static constexpr bool MMA = sizeof(T) == 4 && TB == 128;
+  static constexpr int LDS = MMA ? TB + 4 : TB + 1;  // row stride of a block of T
+  static constexpr int XS = MMA ? 24 : kKC;          // row stride of the staged x
+  static constexpr size_t bytes() {
+    return ((size_t)TB * LDS * sizeof(T) + 15) / 16 * 16 + (size_t)TB * XS * sizeof(T);
+  }
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
 template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE>
 __global__ void __launch_bounds__(TB * 4)
     trsv_chain_kernel(const T* __restrict__ w, int64_t ldw, int n, const T* __restrict__ dinv, T* x, int64_t ldx,
                       int kc, int* flags, int* counter, unsigned* status) {
+  using Lay = ChainLayout<T, TB>;
   constexpr int THREADS = TB * 4;
   constexpr int LPT = TB * TB / THREADS;  // items of a block of T per thread
-  constexpr int LDS = TB + 1;
+  constexpr int LDS = Lay::LDS;
   extern __shared__ uint8_t smraw[];
   T(*lblk)[LDS] = reinterpret_cast<T(*)[LDS]>(smraw);
-  T(*xs)[kKC] = reinterpret_cast<T(*)[kKC]>(smraw + ((size_t)TB * LDS * sizeof(T) + 15) / 16 * 16);
+  T(*xs)[Lay::XS] = reinterpret_cast<T(*)[Lay::XS]>(smraw + ((size_t)TB * LDS * sizeof(T) + 15) / 16 * 16);
   __shared__ int ticket;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nblk = (n + TB - 1) / TB;
   if (tid == 0) ticket = atomicAdd(counter, 1);
   __syncthreads();
   const int t = ticket;
   const int b = LOWER ? t : nblk - 1 - t;
   const int r0 = b * TB, rows = min(TB, n - r0);
-  const int my_r = tid >> 2, my_c = (tid & 3) * 4;
   auto dep = [&](int s) { return LOWER ? s : nblk - 1 - s; };  // the s-th block solved
+  // this thread's four items of the block's sums: (my_r, my_c + i) for the scalar product; for
+  // the tensor-core one, the m16n8 fragment of warp (8 row tiles x 2 column tiles):
+  // rows fr + 8 (i >> 1), columns fc + (i & 1)
+  const int g = lane >> 2, tq = lane & 3;
+  const int fr = 16 * (warp >> 1) + g, fc = 8 * (warp & 1) + 2 * tq;
+  const int my_r = tid >> 2, my_c = (tid & 3) * 4;
+  auto prow = [&](int i) { return Lay::MMA ? fr + 8 * (i >> 1) : my_r; };
+  auto pcol = [&](int i) { return Lay::MMA ? fc + (i & 1) : my_c + i; };
 
   T acc[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int c = my_c + i;
-    acc[i] = (my_r < rows && c < kc) ? x[(int64_t)(r0 + my_r) * ldx + c] : T(0);
+    const int r = prow(i), c = pcol(i);
+    acc[i] = (r < rows && c < kc) ? x[(int64_t)(r0 + r) * ldx + c] : T(0);
   }
   T regs[LPT];
   // a block of T: COLMAJOR storage is read along its columns (coalesced)
@@ -247,19 +281,38 @@ __global__ void __launch_bounds__(TB * 4)
       lblk[e / TB][e % TB] = regs[q];
     }
   };
-  // acc[i] += sign * sum_q lblk[my_r][q] xs[q][my_c + i]
+  // acc += sign * lblk xs (this thread's items)
   auto apply = [&](T sign) {
-#pragma unroll 8
-    for (int q = 0; q < TB; ++q) {
-      const T l = sign * lblk[my_r][q];
+    if constexpr (Lay::MMA) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+      for (int k8 = 0; k8 < TB; k8 += 8) {
+        const float av[4] = {sign * lblk[fr][k8 + tq], sign * lblk[fr + 8][k8 + tq], sign * lblk[fr][k8 + tq + 4],
+                             sign * lblk[fr + 8][k8 + tq + 4]};
+        const float bv0 = xs[k8 + tq][8 * (warp & 1) + g], bv1 = xs[k8 + tq + 4][8 * (warp & 1) + g];
+        uint32_t ah[4], al[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) acc[i] = fma(l, xs[q][my_c + i], acc[i]);
+        for (int i = 0; i < 4; ++i) {
+          ah[i] = to_tf32(av[i]);
+          al[i] = to_tf32(av[i] - __uint_as_float(ah[i]));
+        }
+        const uint32_t bh0 = to_tf32(bv0), bh1 = to_tf32(bv1);
+        const uint32_t bl0 = to_tf32(bv0 - __uint_as_float(bh0)), bl1 = to_tf32(bv1 - __uint_as_float(bh1));
+        mma_tf32_16x8x8(d, al, bh0, bh1);  // the small terms first
+        mma_tf32_16x8x8(d, ah, bl0, bl1);
+        mma_tf32_16x8x8(d, ah, bh0, bh1);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[i] += d[i];
+    } else {
+#pragma unroll 8
+      for (int q = 0; q < TB; ++q) {
+        const T l = sign * lblk[my_r][q];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i] = fma(l, xs[q][my_c + i], acc[i]);
+      }
     }
   };
-  // waits (bounded) for block j's release, then stages x_j in xs
-  // waits (bounded) for block j's release and stages x_j in xs: every thread acquires the flag
-  // itself and loads its share at once, and one barrier (which also agrees on the outcome)
-  // closes the step
   auto fetch = [&](int j) -> bool {
     bool seen = ld_acquire(&flags[j]) != 0;
     if (!seen) {
@@ -288,7 +341,7 @@ __global__ void __launch_bounds__(TB * 4)
     store_mat();
     if (t >= 1) load(dep(0));
 #pragma unroll
-    for (int i = 0; i < 4; ++i) xs[my_r][my_c + i] = acc[i];
+    for (int i = 0; i < 4; ++i) xs[prow(i)][pcol(i)] = acc[i];
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i] = T(0);
@@ -306,8 +359,8 @@ __global__ void __launch_bounds__(TB * 4)
     if (ok) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const int c = my_c + i;
-        if (my_r < rows && c < kc) x[(int64_t)(r0 + my_r) * ldx + c] = acc[i];
+        const int r = prow(i), c = pcol(i);
+        if (r < rows && c < kc) x[(int64_t)(r0 + r) * ldx + c] = acc[i];
       }
     }
   } else {
@@ -329,7 +382,7 @@ __global__ void __launch_bounds__(TB * 4)
     __syncthreads();
     store_mat();
 #pragma unroll
-    for (int i = 0; i < 4; ++i) xs[my_r][my_c + i] = acc[i];
+    for (int i = 0; i < 4; ++i) xs[prow(i)][pcol(i)] = acc[i];
     if (t >= 1) load_mat(2);
     __syncthreads();
 #pragma unroll
@@ -344,8 +397,8 @@ __global__ void __launch_bounds__(TB * 4)
     if (ok) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const int c = my_c + i;
-        if (my_r < rows && c < kc) x[(int64_t)(r0 + my_r) * ldx + c] = acc[i];
+        const int r = prow(i), c = pcol(i);
+        if (r < rows && c < kc) x[(int64_t)(r0 + r) * ldx + c] = acc[i];
       }
     }
   }
@@ -359,7 +412,7 @@ __global__ void __launch_bounds__(TB * 4)
 template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE = false>
 static int launch_trsv(const T* w, int64_t ldw, int n, const T* dinv, T* x, int64_t ldx, int kc, int* flags,
                        int* counter, unsigned* status, cudaStream_t stream) {
-  const size_t smem = ((size_t)TB * (TB + 1) * sizeof(T) + 15) / 16 * 16 + (size_t)TB * kKC * sizeof(T);
+  const size_t smem = ChainLayout<T, TB>::bytes();
   static bool set = false;
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE>,
