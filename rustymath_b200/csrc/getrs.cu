@@ -10,6 +10,7 @@
 // once per factorization by invert_diag_blocks) and publishes its block with a release
 // flag. Waits on flags are bounded: on expiry the status word records a timeout.
 #include "rm_internal.h"
+#include "rm_tcgen05.cuh"
 
 namespace rm {
 
@@ -199,18 +200,6 @@ struct ChainLayout {
   }
 };
 
-__device__ __forceinline__ uint32_t to_tf32(float v) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
-  return r;
-}
-
-__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 
 template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE>
 __global__ void __launch_bounds__(TB * 4)
@@ -293,14 +282,14 @@ __global__ void __launch_bounds__(TB * 4)
         uint32_t ah[4], al[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          ah[i] = to_tf32(av[i]);
-          al[i] = to_tf32(av[i] - __uint_as_float(ah[i]));
+          ah[i] = tc::to_tf32(av[i]);
+          al[i] = tc::to_tf32(av[i] - __uint_as_float(ah[i]));
         }
-        const uint32_t bh0 = to_tf32(bv0), bh1 = to_tf32(bv1);
-        const uint32_t bl0 = to_tf32(bv0 - __uint_as_float(bh0)), bl1 = to_tf32(bv1 - __uint_as_float(bh1));
-        mma_tf32_16x8x8(d, al, bh0, bh1);  // the small terms first
-        mma_tf32_16x8x8(d, ah, bl0, bl1);
-        mma_tf32_16x8x8(d, ah, bh0, bh1);
+        const uint32_t bh0 = tc::to_tf32(bv0), bh1 = tc::to_tf32(bv1);
+        const uint32_t bl0 = tc::to_tf32(bv0 - __uint_as_float(bh0)), bl1 = tc::to_tf32(bv1 - __uint_as_float(bh1));
+        tc::mma_tf32_16x8x8(d, al, bh0, bh1);  // the small terms first
+        tc::mma_tf32_16x8x8(d, ah, bl0, bl1);
+        tc::mma_tf32_16x8x8(d, ah, bh0, bh1);
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[i] += d[i];

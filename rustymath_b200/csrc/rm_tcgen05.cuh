@@ -1,5 +1,7 @@
-// tcgen05 / TMA helpers shared by the tensor-core GEMMs (sgemm_tc.cu, ozaki.cu): shared-
-// memory matrix descriptors, MMA completion, TMEM loads, TMA stores and bulk-group waits.
+// Tensor-core helpers shared by the kernels: for tcgen05 (sgemm_tc.cu, ozaki.cu) shared-memory
+// matrix descriptors, MMA completion, TMEM loads, TMA stores and bulk-group waits; for the
+// warp-level products inside latency-bound kernels (getrs.cu, mixed.cu) TF32 rounding and
+// mma.sync m16n8k8.
 #pragma once
 #include "rm_internal.h"
 
@@ -65,6 +67,36 @@ __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
 }
 __device__ __forceinline__ void tmem_free(uint32_t base, uint32_t cols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(cols));
+}
+
+// x rounded to TF32 (round to nearest, ties away), in a 32-bit register
+__device__ __forceinline__ uint32_t to_tf32(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
+}
+
+// d += A B for a 16 x 8 tile: A 16 x 8 (row), B 8 x 8 (col), TF32 in, float32 accumulate
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// 3xTF32: d += A B with float32-level products (A = Ah + Al, B = Bh + Bl in TF32; Al Bl dropped)
+__device__ __forceinline__ void mma_3xtf32(float (&d)[4], const float (&a)[4], float b0, float b1) {
+  uint32_t ah[4], al[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    ah[i] = to_tf32(a[i]);
+    al[i] = to_tf32(a[i] - __uint_as_float(ah[i]));
+  }
+  const uint32_t bh0 = to_tf32(b0), bh1 = to_tf32(b1);
+  const uint32_t bl0 = to_tf32(b0 - __uint_as_float(bh0)), bl1 = to_tf32(b1 - __uint_as_float(bh1));
+  mma_tf32_16x8x8(d, al, bh0, bh1);  // the small terms first
+  mma_tf32_16x8x8(d, ah, bl0, bl1);
+  mma_tf32_16x8x8(d, ah, bh0, bh1);
 }
 
 }  // namespace tc
