@@ -35,7 +35,7 @@ namespace rm {
 
 constexpr int kLppCols = 128;  // panel width (the trailing update's rank)
 constexpr int kLppRows = 256;  // rows a panel's pivots are chosen among
-constexpr int kLppLeaf = 32;
+constexpr int kLppLeaf = 16;
 constexpr int kLppThreads = 256;  // a thread per row
 constexpr int kLppPRows = 2 * kLppCols;  // rows of the panel buffer (the inverses use its upper half)
 constexpr int kLppStride = kLppCols + 1;
