@@ -120,22 +120,6 @@ __global__ void __launch_bounds__(256) coupling_kernel(const T* __restrict__ w, 
                                  dinv + ((int64_t)b * kDiagMats + 2 + which) * TB * TB, TB);
 }
 
-// pre = the block-Jacobi-scaled triangles of the row-major L\U w: block (b, j) of pre is
-// dinv[b][0] L_bj below the diagonal blocks (j < b) and dinv[b][1] U_bj above them (j > b);
-// the diagonal blocks of pre are not written. With them a triangular solve is
-// x_b = D_b^-1 y_b - sum_j pre_bj x_j: every block's last step is a single product.
-template <typename T, int TB>
-__global__ void __launch_bounds__(256) premultiply_kernel(const T* __restrict__ w, int64_t ldw, int64_t n,
-                                                          const T* __restrict__ dinv, T* __restrict__ pre,
-                                                          int64_t ldp) {
-  const int nblk = (int)((n + TB - 1) / TB);
-  const int b = blockIdx.x / nblk, j = blockIdx.x % nblk;
-  if (b == j) return;
-  const int which = j < b ? 0 : 1;
-  // rows/columns past n land in the padding of pre (ldp >= nblk * TB, rows allocated likewise)
-  block_product<T, false, TB>(w, ldw, n, b, j, dinv + ((int64_t)b * kDiagMats + which) * TB * TB,
-                              pre + (int64_t)b * TB * ldp + (int64_t)j * TB, ldp);
-}
 
 template <typename T, bool COLMAJOR, int TB>
 static int launch_invert(const T* w, int64_t ldw, int64_t n, T* dinv, bool lower_unit, bool upper_unit,
@@ -179,7 +163,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // triangle of the matrix whose item (i, j) is w[i*ldw + j] (w[j*ldw + i] when COLMAJOR),
 // in block rows of TB; dinv holds each block's diagonal inverse and its coupling to the
 // block solved just before it. With PRE, w holds the block-Jacobi-scaled triangles
-// (premultiply_kernel): block b forms D_b^-1 y_b first and subtracts pre_bj x_j as each x_j
+// (premultiply_mma_kernel): block b forms D_b^-1 y_b first and subtracts pre_bj x_j as each x_j
 // is released. flags[nblk] and counter start at zero. CTAs take tickets in
 // launch order and block rows in solve order; block b subtracts T_bj x_j for every block j
 // solved before it but the last, as each x_j is released, then forms z_b = D_b^-1 (...) and,
@@ -536,6 +520,77 @@ int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, 
   return launch_invert<float, false, kTB32>(w, ldw, n, dinv, true, false, stream);
 }
 
+// pre = the block-Jacobi-scaled triangles of the row-major float32 L\U w: block (b, j) of pre is
+// dinv[b][0] L_bj below the diagonal blocks (j < b) and dinv[b][1] U_bj above them (j > b);
+// the diagonal blocks of pre are not written. With them a triangular solve is
+// x_b = D_b^-1 y_b - sum_j pre_bj x_j: every block's last step is a single product.
+// On the tensor cores, for 128-row blocks: out = D_b^-1 T_bj with
+// 3xTF32 mma.sync (float32-level products). 8 warps, warp w the rows 16w .. 16w+15 of all 16
+// column tiles; the operands in padded shared memory (A rows 132 floats apart, B rows 136:
+// both fragment patterns hit 32 distinct banks).
+__global__ void __launch_bounds__(256) premultiply_mma_kernel(const float* __restrict__ w, int64_t ldw, int64_t n,
+                                                              const float* __restrict__ dinv, float* __restrict__ pre,
+                                                              int64_t ldp) {
+  constexpr int TB = 128, SA = 132, SB = 136;
+  extern __shared__ uint8_t smraw[];
+  float(*di)[SA] = reinterpret_cast<float(*)[SA]>(smraw);
+  float(*ob)[SB] = reinterpret_cast<float(*)[SB]>(smraw + (size_t)TB * SA * sizeof(float));
+  const int nblk = (int)((n + TB - 1) / TB);
+  const int b = blockIdx.x / nblk, j = blockIdx.x % nblk;
+  if (b == j) return;
+  const int which = j < b ? 0 : 1;
+  const int64_t r0 = (int64_t)b * TB, c0 = (int64_t)j * TB;
+  const float* dv = dinv + ((int64_t)b * kDiagMats + which) * TB * TB;
+  {
+    // both operands as 16-byte loads, all 32 of a thread's in flight before any store
+    constexpr int PER = TB * TB / 4 / 256;  // float4 items per thread and operand
+    float4 va[PER], vb[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = (threadIdx.x + q * 256) * 4;
+      const int i = e / TB, c = e % TB;
+      va[q] = __ldg(reinterpret_cast<const float4*>(dv + e));
+      const int64_t gi = r0 + i, gj = c0 + c;
+      const float* src = w + gi * ldw + gj;
+      if (gi < n && gj + 3 < n) {
+        vb[q] = __ldcs(reinterpret_cast<const float4*>(src));
+      } else {
+        vb[q].x = (gi < n && gj < n) ? src[0] : 0.0f;
+        vb[q].y = (gi < n && gj + 1 < n) ? src[1] : 0.0f;
+        vb[q].z = (gi < n && gj + 2 < n) ? src[2] : 0.0f;
+        vb[q].w = (gi < n && gj + 3 < n) ? src[3] : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = (threadIdx.x + q * 256) * 4;
+      const int i = e / TB, c = e % TB;
+      *reinterpret_cast<float4*>(&di[i][c]) = va[q];
+      *reinterpret_cast<float4*>(&ob[i][c]) = vb[q];
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+  const int ra = 16 * warp + g;
+  float d[16][4];
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) d[nt][e] = 0.f;
+  for (int k8 = 0; k8 < TB; k8 += 8) {
+    const float a[4] = {di[ra][k8 + tq], di[ra + 8][k8 + tq], di[ra][k8 + tq + 4], di[ra + 8][k8 + tq + 4]};
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) tc::mma_3xtf32(d[nt], a, ob[k8 + tq][8 * nt + g], ob[k8 + tq + 4][8 * nt + g]);
+  }
+  float* out = pre + r0 * ldp + c0;
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    const int col = 8 * nt + 2 * tq;
+    *reinterpret_cast<float2*>(out + (int64_t)ra * ldp + col) = make_float2(d[nt][0], d[nt][1]);
+    *reinterpret_cast<float2*>(out + (int64_t)(ra + 8) * ldp + col) = make_float2(d[nt][2], d[nt][3]);
+  }
+}
+
 int64_t premultiplied_f32_ld(int64_t n) { return (n + kTB32 - 1) / kTB32 * kTB32; }
 size_t premultiplied_f32_bytes(int64_t n) {
   const int64_t ld = premultiplied_f32_ld(n);
@@ -545,15 +600,13 @@ size_t premultiplied_f32_bytes(int64_t n) {
 int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, float* pre, cudaStream_t stream) {
   const int nblk = (int)((n + kTB32 - 1) / kTB32);
   if (nblk < 2) return RM_OK;
-  const size_t smem = 2 * (size_t)kTB32 * (kTB32 + 1) * sizeof(float);
+  const size_t smem = (size_t)kTB32 * (132 + 136) * sizeof(float);
   static bool set = false;
   if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(premultiply_kernel<float, kTB32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+    RM_CUDA_TRY(cudaFuncSetAttribute(premultiply_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     set = true;
   }
-  premultiply_kernel<float, kTB32><<<nblk * nblk, 256, smem, stream>>>(lu, ld, n, dinv, pre,
-                                                                        premultiplied_f32_ld(n));
+  premultiply_mma_kernel<<<nblk * nblk, 256, smem, stream>>>(lu, ld, n, dinv, pre, premultiplied_f32_ld(n));
   RM_LAUNCHED();
   return RM_OK;
 }
