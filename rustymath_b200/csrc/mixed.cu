@@ -94,7 +94,7 @@ __device__ __forceinline__ unsigned pivot_key(float v) {
 __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __restrict__ a, int64_t lda, int j0, int nb,
                                                                 int T, float* __restrict__ linv,
                                                                 float* __restrict__ uinvt, int* __restrict__ plocal,
-                                                                unsigned* status) {
+                                                                float* __restrict__ dblk, unsigned* status) {
   extern __shared__ float sm[];
   float(*P)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm);
   float(*X)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm + kLppPRows * kLppStride);
@@ -332,9 +332,15 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
   }
   for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32)
     for (int c = lane; c < kLppCols; c += 32) {
-      linv[rr * kLppCols + c] = rr >= c ? XL[rr][c] : 0.0f;
-      uinvt[rr * kLppCols + c] = rr >= c ? XU[rr][c] : 0.0f;
+      const float l = rr >= c ? XL[rr][c] : 0.0f, u = rr >= c ? XU[rr][c] : 0.0f;
+      linv[rr * kLppCols + c] = l;
+      uinvt[rr * kLppCols + c] = u;
+      if (dblk) dblk[rr * kLppCols + c] = l;  // the triangular solves' table: L11^-1 ...
     }
+  if (dblk)  // ... and U11^-1 row-major (XU's transpose), lanes along the output rows
+    for (int c = warp; c < kLppCols; c += kLppThreads / 32)
+      for (int rr = lane; rr < kLppCols; rr += 32)
+        dblk[kLppCols * kLppCols + c * kLppCols + rr] = rr >= c ? XU[rr][c] : 0.0f;
 }
 
 constexpr size_t kLppSmem = ((size_t)(kLppPRows + kLppCols) * kLppStride + 3 * 32 * 33) * sizeof(float);
@@ -422,7 +428,8 @@ size_t getrf_lpp_f32_scratch_bytes(int64_t n) {
          2048;
 }
 
-int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, unsigned* status, cudaStream_t stream) {
+int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, unsigned* status, cudaStream_t stream,
+                  float* dinv) {
   if (n <= 0) return RM_OK;
   if (n > INT32_MAX / 2) return RM_BAD_ARG;
   float* linv = reinterpret_cast<float*>(scratch);
@@ -449,7 +456,8 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
     const int T = std::min(kLppRows, ni - J0);
     const int J1 = J0 + nb;
     const int rest = ni - J1;
-    lpp_panel_kernel<<<1, kLppThreads, kLppSmem, stream>>>(a, lda, J0, nb, T, linv, uinvt, plocal, status);
+    float* dblk = dinv ? dinv + (size_t)(J0 / kLppCols) * kDiagMats * kLppCols * kLppCols : nullptr;
+    lpp_panel_kernel<<<1, kLppThreads, kLppSmem, stream>>>(a, lda, J0, nb, T, linv, uinvt, plocal, dblk, status);
     RM_LAUNCHED();
     if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
     const int chunks = (J0 + kApplyCols - 1) / kApplyCols + (rest + kApplyCols - 1) / kApplyCols;

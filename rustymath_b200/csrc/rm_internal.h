@@ -113,7 +113,10 @@ int dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double* a, int64_t lda, c
 size_t getrf_lpp_f32_scratch_bytes(int64_t n);
 // float32 LU of the row-major n x n a (lda % 4 == 0) with each 128-column panel pivoted among
 // its own 256 rows; perm[i] (int32) = the row of the input that row i of L U comes from.
-int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, unsigned* status, cudaStream_t stream);
+// dinv (optional): the diagonal blocks' inverses L11^-1, U11^-1 of each 128-column panel go to
+// its slots [b][0], [b][1] of the triangular solves' table (kDiagMats matrices of 128^2 per block)
+int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, unsigned* status, cudaStream_t stream,
+                  float* dinv = nullptr);
 int to_f32(const double* a, int64_t lda, int64_t n, float* f, int64_t ldf, cudaStream_t stream);
 // c (float32) = r[perm]; x (float64) = c or x += c.
 int gather_f32(const double* r, int64_t ldr, const int* perm, int64_t n, int64_t k, float* c, int64_t ldc,
