@@ -18,11 +18,14 @@
 // and the fallback answers.
 //
 // Per 128-column panel at J0 (T = min(256, n - J0) rows):
-//   lpp_panel_kernel : GEPP of the T x 128 panel among its T rows, in 32-column leaves with
-//                      a shared-memory block update between leaves; writes L11^-1,
-//                      (U11^-1)^T and the panel's row permutation
-//   lpp_apply_kernel : that permutation on every other column of rows J0..J0+T, A12^T into
+//   lpp_panel_kernel : GEPP of the T x 128 panel among its T rows, in 16-column leaves with
+//                      a shared-memory block update between leaves, and the panel's row
+//                      permutation
+//   lpp_post_kernel  : L11^-1 and (U11^-1)^T (a 32-column block per CTA), beside the
+//                      permutation of the columns right of the panel and A12^T into
 //                      a buffer, and the global permutation
+//   lpp_apply_kernel : the permutation of the columns left of the panel (off the critical
+//                      path: nothing reads them again during the factorization)
 //   sgemm_tc         : U12^T = A12^T (L11^-1)^T, written both to a buffer and over A12
 //   sgemm_tc         : L21 = A21 U11^-1 for the rows below the panel, in place
 //   sgemm_tc         : A22 -= L21 U12
@@ -37,7 +40,6 @@ constexpr int kLppCols = 128;  // panel width (the trailing update's rank)
 constexpr int kLppRows = 256;  // rows a panel's pivots are chosen among
 constexpr int kLppLeaf = 16;
 constexpr int kLppThreads = 256;  // a thread per row
-constexpr int kLppPRows = 2 * kLppCols;  // rows of the panel buffer (the inverses use its upper half)
 constexpr int kLppStride = kLppCols + 1;
 
 __device__ __forceinline__ void warp_argmax_f32(float& v, int& i) {
@@ -65,11 +67,11 @@ __global__ void to_f32_kernel(const double* __restrict__ a, int64_t lda, int64_t
 // ------------------------------------------------------------------ the panel
 struct alignas(16) LppSlot {
   float row[kLppLeaf];  // a warp's candidate pivot row (its current leaf columns)
-  unsigned key;         // its |pivot| as an ordered key: bits + 2; 1 for NaN; 0: no candidate
   int idx;              // its row
   float rcp;            // 1 / pivot
-  int pad;
+  int pad[2];
 };
+static_assert(kLppThreads == 256, "the pivot search reduces 8 warp posts");
 
 // |v| as an unsigned key ordered like the magnitudes: 0 is no candidate, 1 a NaN (never chosen
 // over a number), otherwise the float's bits + 2 (non-negative floats order like their bits).
@@ -81,27 +83,26 @@ __device__ __forceinline__ unsigned pivot_key(float v) {
 // Factors the T x nb panel A[j0.., j0..] (T <= 256, nb <= 128) with partial pivoting among
 // its T rows. Thread r owns row r. Pivoting is implicit: rows stay where they are and a row
 // chosen as a pivot leaves the candidates; the panel is written back in pivot order at the
-// end. Within a 32-column leaf each thread keeps its row's leaf in registers, and each
-// column costs one barrier: every warp posts its best candidate and that candidate's row, and
-// after the barrier every thread picks the winner among 8 posts (largest |pivot|, first row
-// on ties, NaN never chosen over a number) and reads the pivot row from it (two buffers of
-// posts alternate between columns, so a column's posts are never overwritten while read).
+// end. Within a 16-column leaf each thread keeps its row's leaf in registers, and each
+// column costs one barrier: every warp posts its best candidate (redux.sync max of the keys,
+// the lowest lane holding it by ballot), that candidate's row and reciprocal, and after the
+// barrier every thread reads the 8 keys (two 16-byte loads) and picks the winner by a
+// three-level compare tree in registers (largest |pivot|, lowest warp and so first row on
+// ties, NaN never chosen over a number), then reads the pivot row from its post (two
+// buffers of posts alternate between columns, so a column's posts are never overwritten
+// while read).
 // After a leaf: U12 of its pivot rows (unit-lower solve, a column per thread) and the block
 // update of the later columns of the rows still unchosen. Then the pivot rows come first in
 // choice order and the others follow in their original order: plocal[i] is the panel row
-// that row i came from; linv = L11^-1 and uinvt = (U11^-1)^T (ld 128). A zero pivot sets
-// RM_DEV_NAN and leaves its column unreduced.
+// that row i came from. A zero pivot sets RM_DEV_NAN and leaves its column unreduced.
 __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __restrict__ a, int64_t lda, int j0, int nb,
-                                                                int T, float* __restrict__ linv,
-                                                                float* __restrict__ uinvt, int* __restrict__ plocal,
-                                                                float* __restrict__ dblk, unsigned* status) {
+                                                                int T, int* __restrict__ plocal, unsigned* status) {
   extern __shared__ float sm[];
   float(*P)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm);
-  float(*X)[kLppStride] = reinterpret_cast<float(*)[kLppStride]>(sm + kLppPRows * kLppStride);
-  float(*Tm)[33] = reinterpret_cast<float(*)[33]>(sm + (kLppPRows + kLppCols) * kLppStride);  // 96 x 33
-  // during the factorization X's space holds the leaf's U12, transposed (column j's 32 values contiguous)
-  float(*UbT)[kLppLeaf + 4] = reinterpret_cast<float(*)[kLppLeaf + 4]>(X);
+  // the leaf's U12, transposed (column j's 16 values contiguous)
+  float(*UbT)[kLppLeaf + 4] = reinterpret_cast<float(*)[kLppLeaf + 4]>(sm + kLppRows * kLppStride);
   __shared__ LppSlot slot[2][kLppThreads / 32];
+  __shared__ __align__(16) unsigned skey[2][kLppThreads / 32];  // the posts' keys
   __shared__ __align__(16) float Lp[kLppLeaf][kLppLeaf + 4];
   __shared__ int piv_s[kLppCols];
   __shared__ int order_s[kLppRows];
@@ -109,13 +110,38 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r = tid;
   float* blk = a + (int64_t)j0 * lda + j0;
-  for (int e = tid; e < T * nb; e += kLppThreads) {
-    const int rr = e / nb, c = e % nb;
-    P[rr][c] = blk[(int64_t)rr * lda + c];
+  if (nb == kLppCols) {
+    // a warp per row, a 16-byte load per lane, eight rows in flight; lane q stores its four
+    // floats rotated by q / 8 so that the stores of a warp hit 32 distinct banks
+    const int rot = lane >> 3;
+    for (int r0 = warp; r0 < T; r0 += 8 * (kLppThreads / 32)) {
+      float4 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int rr = r0 + u * (kLppThreads / 32);
+        v[u] = rr < T ? *reinterpret_cast<const float4*>(blk + (int64_t)rr * lda + 4 * lane) : make_float4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int rr = r0 + u * (kLppThreads / 32);
+        if (rr < T) {
+          const float e[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const int q = (t + rot) & 3;
+            P[rr][4 * lane + q] = q == 0 ? e[0] : q == 1 ? e[1] : q == 2 ? e[2] : e[3];
+          }
+        }
+      }
+    }
+  } else {
+    for (int e = tid; e < T * nb; e += kLppThreads) {
+      const int rr = e / nb, c = e % nb;
+      P[rr][c] = blk[(int64_t)rr * lda + c];
+    }
   }
   bool active = r < T;
   __syncthreads();
-
   for (int L = 0; L * kLppLeaf < nb; ++L) {
     const int c0 = L * kLppLeaf;
     const bool was_active = active;
@@ -126,26 +152,36 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
     for (int c = 0; c < kLppLeaf; ++c) {
       if (c0 + c >= nb) continue;  // the last panel may be narrower than a leaf
       LppSlot* sl = &slot[c & 1][0];
-      // the warp's candidate: the largest key (redux), the lowest lane holding it (ballot)
+      // the warp's candidate: the largest key (redux), the lowest lane holding it (ballot);
+      // every lane's reciprocal is taken while the reduction runs, the winner posts its own
       const unsigned key = active ? pivot_key(p[c]) : 0u;
+      const float myrcp = __frcp_rn(p[c]);
       const unsigned wmax = __reduce_max_sync(0xffffffffu, key);
       const int wl = __ffs(__ballot_sync(0xffffffffu, key == wmax)) - 1;
       if (lane == wl) {
         float4* dst = reinterpret_cast<float4*>(sl[warp].row);
 #pragma unroll
         for (int i = 0; i < kLppLeaf / 4; ++i) dst[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
-        sl[warp].key = wmax;
-        sl[warp].idx = r;
-        sl[warp].rcp = __frcp_rn(p[c]);
+        *reinterpret_cast<int2*>(&sl[warp].idx) = make_int2(r, __float_as_int(myrcp));
+        skey[c & 1][warp] = wmax;
       }
       __syncthreads();
       // the winning post: the largest key, the lowest warp (so the lowest row) among equals
-      const unsigned kq = lane < kLppThreads / 32 ? sl[lane].key : 0u;
-      const unsigned gmax = __reduce_max_sync(0xffffffffu, kq);
-      const unsigned gball = __ballot_sync(0xffffffffu, lane < kLppThreads / 32 && kq == gmax);
-      const int bw = gball ? __ffs(gball) - 1 : 0;
-      const int bi = sl[bw].idx;
-      const float prcp = sl[bw].rcp;
+      int bw;
+      {
+        const uint4 k0 = *reinterpret_cast<const uint4*>(&skey[c & 1][0]);
+        const uint4 k1 = *reinterpret_cast<const uint4*>(&skey[c & 1][4]);
+        const bool s0 = k0.x >= k0.y, s1 = k0.z >= k0.w, s2 = k1.x >= k1.y, s3 = k1.z >= k1.w;
+        const unsigned a0 = s0 ? k0.x : k0.y, a1 = s1 ? k0.z : k0.w, a2 = s2 ? k1.x : k1.y, a3 = s3 ? k1.z : k1.w;
+        const int w0 = s0 ? 0 : 1, w1 = s1 ? 2 : 3, w2 = s2 ? 4 : 5, w3 = s3 ? 6 : 7;
+        const bool t0 = a0 >= a1, t1 = a2 >= a3;
+        const unsigned b0 = t0 ? a0 : a1, b1 = t1 ? a2 : a3;
+        const int v0 = t0 ? w0 : w1, v1 = t1 ? w2 : w3;
+        bw = b0 >= b1 ? v0 : v1;
+      }
+      const int2 meta = *reinterpret_cast<const int2*>(&sl[bw].idx);
+      const int bi = meta.x;
+      const float prcp = __int_as_float(meta.y);
       // the pivot row, as 16-byte reads of the winning post
       float prow[kLppLeaf];
       {
@@ -237,142 +273,156 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
     float* dst = blk + (int64_t)rr * lda;
     for (int c = lane; c < nb; c += 32) dst[c] = src[c];
   }
-  // ---- the inverses. D (P's rows 0..127) = the diagonal block in pivot order: L11 below its
-  // diagonal (unit), U11 on and above it. XL (X's space) = L11^-1 and XU (P's rows 128..) =
-  // (U11^T)^-1 = (U11^-1)^T are both lower triangles, built the same way: the diagonal 32 x 32
-  // blocks first (a warp each, a lane per column, zeros above their diagonals), then the
-  // blocks below in order of distance b - a = gap: T = sum_{c=a..b-1} M_bc X_ca in Tm,
-  // X_ba = -X_bb T, each thread a 2 x 2 piece of every block of a gap. M_0(i, k) = D[i][k],
-  // M_1(i, k) = D[k][i].
-  float(*D)[kLppStride] = P;
-  float(*XL)[kLppStride] = X;
-  float(*XU)[kLppStride] = P + kLppCols;
-  for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32) {
-    const float* src = P[rr < nb ? order_s[rr] : 0];
-    for (int c = lane; c < kLppCols; c += 32) X[rr][c] = (rr < nb && c < nb) ? src[c] : (rr == c ? 1.0f : 0.0f);
-  }
-  __syncthreads();
-  for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32)
-    for (int c = lane; c < kLppCols; c += 32) D[rr][c] = X[rr][c];
-  __syncthreads();
-  for (int job = warp; job < 8; job += kLppThreads / 32) {  // 4 blocks of L11, then 4 of U11^T
-    const int b0 = (job & 3) * 32;
-    float x[32];
-    if (job < 4) {
-#pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        float acc = i == lane ? 1.0f : 0.0f;
-#pragma unroll
-        for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + i][b0 + k2], x[k2], acc);
-        x[i] = i < lane ? 0.0f : acc;
-      }
-#pragma unroll
-      for (int i = 0; i < 32; ++i) XL[b0 + i][b0 + lane] = x[i];
-    } else {
-#pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        float acc = i == lane ? 1.0f : 0.0f;
-#pragma unroll
-        for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-D[b0 + k2][b0 + i], x[k2], acc);
-        x[i] = i < lane ? 0.0f : acc / D[b0 + i][b0 + i];
-      }
-#pragma unroll
-      for (int i = 0; i < 32; ++i) XU[b0 + i][b0 + lane] = x[i];
-    }
-  }
-  __syncthreads();
-  {
-    float(*Tq)[33] = Tm;  // up to 3 blocks of 32 x 33
-    for (int gap = 1; gap < 4; ++gap)
-      for (int m = 0; m < 2; ++m) {
-        float(*Xm)[kLppStride] = m == 0 ? XL : XU;
-        for (int a = 0; a + gap < 4; ++a) {
-          const int b = a + gap;
-          for (int tp = tid; tp < 256; tp += kLppThreads) {  // rows ti, ti+16, columns tj, tj+16
-            const int ti = tp >> 4, tj = tp & 15;
-            float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
-            const int r0 = 32 * b + ti, r1 = r0 + 16, c0 = 32 * a + tj, c1 = c0 + 16;
-            if (m == 0) {
-#pragma unroll 4
-              for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
-                const float m0 = D[r0][k2], m1 = D[r1][k2], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
-                t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
-              }
-            } else {
-#pragma unroll 4
-              for (int k2 = 32 * a; k2 < 32 * b; ++k2) {
-                const float m0 = D[k2][r0], m1 = D[k2][r1], x0 = Xm[k2][c0], x1 = Xm[k2][c1];
-                t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
-              }
-            }
-            float(*T1)[33] = Tq + 32 * a;
-            T1[ti][tj] = t00, T1[ti][tj + 16] = t01, T1[ti + 16][tj] = t10, T1[ti + 16][tj + 16] = t11;
-          }
-        }
-        __syncthreads();
-        for (int a = 0; a + gap < 4; ++a) {
-          const int b = a + gap;
-          float(*T1)[33] = Tq + 32 * a;
-          for (int tp = tid; tp < 256; tp += kLppThreads) {
-            const int ti = tp >> 4, tj = tp & 15;
-            float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
-            const int r0 = 32 * b + ti, r1 = r0 + 16;
-#pragma unroll 4
-            for (int k2 = 0; k2 < 32; ++k2) {
-              const float x0 = Xm[r0][32 * b + k2], x1 = Xm[r1][32 * b + k2];
-              const float u0 = T1[k2][tj], u1 = T1[k2][tj + 16];
-              t00 = fmaf(x0, u0, t00), t01 = fmaf(x0, u1, t01), t10 = fmaf(x1, u0, t10), t11 = fmaf(x1, u1, t11);
-            }
-            Xm[r0][32 * a + tj] = -t00, Xm[r0][32 * a + tj + 16] = -t01, Xm[r1][32 * a + tj] = -t10,
-                            Xm[r1][32 * a + tj + 16] = -t11;
-          }
-        }
-        __syncthreads();
-      }
-  }
-  for (int rr = warp; rr < kLppCols; rr += kLppThreads / 32)
-    for (int c = lane; c < kLppCols; c += 32) {
-      const float l = rr >= c ? XL[rr][c] : 0.0f, u = rr >= c ? XU[rr][c] : 0.0f;
-      linv[rr * kLppCols + c] = l;
-      uinvt[rr * kLppCols + c] = u;
-      if (dblk) dblk[rr * kLppCols + c] = l;  // the triangular solves' table: L11^-1 ...
-    }
-  if (dblk)  // ... and U11^-1 row-major (XU's transpose), lanes along the output rows
-    for (int c = warp; c < kLppCols; c += kLppThreads / 32)
-      for (int rr = lane; rr < kLppCols; rr += 32)
-        dblk[kLppCols * kLppCols + c * kLppCols + rr] = rr >= c ? XU[rr][c] : 0.0f;
 }
 
-constexpr size_t kLppSmem = ((size_t)(kLppPRows + kLppCols) * kLppStride + 3 * 32 * 33) * sizeof(float);
+constexpr size_t kLppSmem = ((size_t)kLppRows * kLppStride + (size_t)kLppCols * (kLppLeaf + 4)) * sizeof(float);
+
+// ------------------------------------------------------------------ the diagonal block's inverses
+// X = M^-1 for the lower triangles M = L11 (unit; m = 0) and M = U11^T (m = 1) of the panel's
+// factored diagonal block (rows j0.. of a in pivot order, nb x nb; identity beyond nb). CTA
+// (m, a) builds X's 32-column block a: X_aa = M_aa^-1, then block row by block row
+// X_ba = -M_bb^-1 sum_{c=a..b-1} M_bc X_ca. The diagonal blocks' inverses come first, a warp
+// each, a lane per column (forward substitution). Outputs: linv = L11^-1 and
+// uinvt = (U11^-1)^T (ld 128), and when dblk is not NULL L11^-1 and U11^-1 row-major as the
+// triangular solves' table entries [0] and [1] of this block.
+constexpr int kInvStride = kLppCols + 1;
+constexpr size_t kInvSmem = ((size_t)kLppCols * kInvStride + (4 * 32 + kLppCols + 32) * 33) * sizeof(float);
+
+__device__ __forceinline__ void lpp_inverse_block(float* sm, int bid, const float* __restrict__ a, int64_t lda,
+                                                  int j0, int nb, float* __restrict__ linv, float* __restrict__ uinvt,
+                                                  float* __restrict__ dblk) {
+  float(*M)[kInvStride] = reinterpret_cast<float(*)[kInvStride]>(sm);        // rows, columns >= a0 used
+  float(*Y)[33] = reinterpret_cast<float(*)[33]>(sm + kLppCols * kInvStride);  // M_bb^-1 at rows 32 b
+  float(*X)[33] = Y + 4 * 32;                                                  // the column block
+  float(*Tq)[33] = X + kLppCols;                                               // 32 x 33
+  const int m = bid >> 2, ab = bid & 3, a0 = 32 * ab;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float* blk = a + (int64_t)j0 * lda + j0;
+  // M from row a0 on: a warp per stored row, lanes along it
+  if (nb == kLppCols) {
+    // a 16-byte load per lane, all of a thread's rows in flight; lane l stores its four floats
+    // rotated by l / 8, so that the stores of a warp hit 32 distinct banks
+    const int rot = lane >> 3;
+    float4 v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int i = a0 + warp + 8 * u;
+      v[u] = i < kLppCols ? *reinterpret_cast<const float4*>(blk + (int64_t)i * lda + 4 * lane) : make_float4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int i = a0 + warp + 8 * u;
+      if (i < kLppCols) {
+        const float e[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int q = (t + rot) & 3;
+          const float x = q == 0 ? e[0] : q == 1 ? e[1] : q == 2 ? e[2] : e[3];
+          if (m == 0) M[i][4 * lane + q] = x;
+          else M[4 * lane + q][i] = x;
+        }
+      }
+    }
+  } else {
+    for (int i = a0 + warp; i < kLppCols; i += 8)
+      for (int k = a0 + lane; k < kLppCols; k += 32) {
+        const float v = (i < nb && k < nb) ? blk[(int64_t)i * lda + k] : (i == k ? 1.0f : 0.0f);
+        if (m == 0) M[i][k] = v;
+        else M[k][i] = v;
+      }
+  }
+  __syncthreads();
+  if (warp < 4 - ab) {  // Y_b = M_bb^-1, b = ab + warp
+    const int b0 = a0 + 32 * warp;
+    float x[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      float acc = i == lane ? 1.0f : 0.0f;
+#pragma unroll
+      for (int k2 = 0; k2 < i; ++k2) acc = fmaf(-M[b0 + i][b0 + k2], x[k2], acc);
+      x[i] = i < lane ? 0.0f : (m == 0 ? acc : acc / M[b0 + i][b0 + i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) Y[b0 + i][lane] = x[i];
+  }
+  __syncthreads();
+  for (int e = tid; e < 32 * 32; e += 256) X[a0 + (e >> 5)][e & 31] = Y[a0 + (e >> 5)][e & 31];
+  __syncthreads();
+  const int ti = tid >> 4, tj = tid & 15;  // rows ti, ti + 16 and columns tj, tj + 16 of a 32 x 32 block
+  for (int b = ab + 1; b < 4; ++b) {
+    const int r0 = 32 * b + ti, r1 = r0 + 16;
+    float t00 = 0.f, t01 = 0.f, t10 = 0.f, t11 = 0.f;
+#pragma unroll 4
+    for (int k = a0; k < 32 * b; ++k) {
+      const float m0 = M[r0][k], m1 = M[r1][k], x0 = X[k][tj], x1 = X[k][tj + 16];
+      t00 = fmaf(m0, x0, t00), t01 = fmaf(m0, x1, t01), t10 = fmaf(m1, x0, t10), t11 = fmaf(m1, x1, t11);
+    }
+    Tq[ti][tj] = t00, Tq[ti][tj + 16] = t01, Tq[ti + 16][tj] = t10, Tq[ti + 16][tj + 16] = t11;
+    __syncthreads();
+    t00 = t01 = t10 = t11 = 0.f;
+#pragma unroll 4
+    for (int k2 = 0; k2 < 32; ++k2) {
+      const float y0 = Y[r0][k2], y1 = Y[r1][k2], u0 = Tq[k2][tj], u1 = Tq[k2][tj + 16];
+      t00 = fmaf(y0, u0, t00), t01 = fmaf(y0, u1, t01), t10 = fmaf(y1, u0, t10), t11 = fmaf(y1, u1, t11);
+    }
+    X[r0][tj] = -t00, X[r0][tj + 16] = -t01, X[r1][tj] = -t10, X[r1][tj + 16] = -t11;
+    __syncthreads();
+  }
+  // rows above a0 are zero; X is lower triangular within block a (zeros above the diagonal)
+  float* out = m == 0 ? linv : uinvt;
+  for (int rr = warp; rr < kLppCols; rr += 8) {
+    const float v = rr >= a0 ? X[rr][lane] : 0.0f;
+    out[rr * kLppCols + a0 + lane] = v;
+    if (dblk && m == 0) dblk[rr * kLppCols + a0 + lane] = v;
+  }
+  if (dblk && m == 1)  // U11^-1 = X^T row-major: row a0 + c holds X's column c, lanes along it
+    for (int c = warp; c < 32; c += 8)
+      for (int rr = lane; rr < kLppCols; rr += 32)
+        dblk[kLppCols * kLppCols + (a0 + c) * kLppCols + rr] = rr >= a0 ? X[rr][c] : 0.0f;
+}
 
 // ------------------------------------------------------------------ the panel's row permutation
 constexpr int kApplyCols = 32;
+constexpr size_t kApplySmem = (size_t)kLppRows * (kApplyCols + 1) * sizeof(float) + kLppRows * sizeof(int);
 
-// Rows j0..j0+T of the columns [0, j0) and [j1, n) take the panel's permutation (new row i =
-// old row plocal[i]); for columns >= j1 the first nb new rows also go, transposed, to a12t
-// (ld 128). Block 0 also permutes perm[j0..j0+T).
-__global__ void __launch_bounds__(256) lpp_apply_kernel(float* __restrict__ a, int64_t lda, int n, int j0, int j1,
-                                                        int T, const int* __restrict__ plocal, float* __restrict__ a12t,
-                                                        int* __restrict__ perm) {
-  __shared__ float buf[kLppRows][kApplyCols + 1];
-  __shared__ int pl[kLppRows];
+// Rows j0..j0+T of a band of columns take the panel's permutation (new row i = old row
+// plocal[i]): the columns [j1, n) when right, else [0, j0), 32 columns per CTA. For the right
+// band the first nb new rows also go, transposed, to a12t (ld 128), and block 0 permutes
+// perm[j0..j0+T). A full 32-column chunk moves as 16-byte accesses, eight per thread in flight:
+// thread t covers rows t/8 + 32u and the chunk's float4 t%8, so the shared-memory stores of a
+// warp (4 rows x 8 float4 at stride 33) hit 32 distinct banks.
+__device__ __forceinline__ void lpp_apply_band(float* sm, int bid, float* __restrict__ a, int64_t lda, int n, int j0,
+                                               int j1, int T, const int* __restrict__ plocal,
+                                               float* __restrict__ a12t, int* __restrict__ perm, bool right) {
+  float(*buf)[kApplyCols + 1] = reinterpret_cast<float(*)[kApplyCols + 1]>(sm);
+  int* pl = reinterpret_cast<int*>(sm + kLppRows * (kApplyCols + 1));
   const int tid = threadIdx.x;
   if (tid < T) pl[tid] = plocal[tid];
   __syncthreads();
-  const int left_chunks = (j0 + kApplyCols - 1) / kApplyCols;
-  int c0, c1;
-  bool right;
-  if ((int)blockIdx.x < left_chunks) {
-    c0 = blockIdx.x * kApplyCols;
-    c1 = min(c0 + kApplyCols, j0);
-    right = false;
-  } else {
-    c0 = j1 + (blockIdx.x - left_chunks) * kApplyCols;
-    c1 = min(c0 + kApplyCols, n);
-    right = true;
-  }
+  const int c0 = right ? j1 + bid * kApplyCols : bid * kApplyCols;
+  const int c1 = min(c0 + kApplyCols, right ? n : j0);
   const int w = c1 - c0;
-  if (w > 0) {
+  if (w == kApplyCols) {
+    const int q = tid & 7, rb = tid >> 3;
+    float4 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int r = rb + 32 * u;
+      v[u] = r < T ? *reinterpret_cast<const float4*>(a + (int64_t)(j0 + pl[r]) * lda + c0 + 4 * q)
+                   : make_float4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int r = rb + 32 * u;
+      if (r < T) buf[r][4 * q] = v[u].x, buf[r][4 * q + 1] = v[u].y, buf[r][4 * q + 2] = v[u].z, buf[r][4 * q + 3] = v[u].w;
+    }
+    __syncthreads();  // every source row is read before any is overwritten
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int r = rb + 32 * u;
+      if (r < T && pl[r] != r) *reinterpret_cast<float4*>(a + (int64_t)(j0 + r) * lda + c0 + 4 * q) = v[u];
+    }
+  } else if (w > 0) {
     for (int e = tid; e < T * kApplyCols; e += 256) {
       const int r = e / kApplyCols, c = e % kApplyCols;
       if (c < w) buf[r][c] = a[(int64_t)(j0 + pl[r]) * lda + c0 + c];
@@ -382,20 +432,38 @@ __global__ void __launch_bounds__(256) lpp_apply_kernel(float* __restrict__ a, i
       const int r = e / kApplyCols, c = e % kApplyCols;
       if (c < w && pl[r] != r) a[(int64_t)(j0 + r) * lda + c0 + c] = buf[r][c];
     }
-    if (right) {
-      const int nb = j1 - j0;
-      for (int e = tid; e < nb * kApplyCols; e += 256) {
-        const int c = e / nb, r = e % nb;  // consecutive threads: consecutive rows of a12t's row
-        if (c < w) a12t[(int64_t)(c0 - j1 + c) * kLppCols + r] = buf[r][c];
-      }
+  }
+  if (right) {
+    __syncthreads();
+    const int nb = j1 - j0;
+    for (int e = tid; e < nb * kApplyCols; e += 256) {
+      const int c = e / nb, r = e % nb;  // consecutive threads: consecutive rows of a12t's row
+      if (c < w) a12t[(int64_t)(c0 - j1 + c) * kLppCols + r] = buf[r][c];
+    }
+    if (bid == 0) {
+      const int v = tid < T ? perm[j0 + pl[tid]] : 0;
+      __syncthreads();
+      if (tid < T) perm[j0 + tid] = v;
     }
   }
-  if (blockIdx.x == 0) {
-    __syncthreads();
-    const int v = tid < T ? perm[j0 + pl[tid]] : 0;
-    __syncthreads();
-    if (tid < T) perm[j0 + tid] = v;
-  }
+}
+
+// The left band of a panel's row permutation, 32 columns per CTA.
+__global__ void __launch_bounds__(256) lpp_apply_kernel(float* __restrict__ a, int64_t lda, int n, int j0, int j1,
+                                                        int T, const int* __restrict__ plocal) {
+  extern __shared__ float sm[];
+  lpp_apply_band(sm, blockIdx.x, a, lda, n, j0, j1, T, plocal, nullptr, nullptr, false);
+}
+
+// What follows a panel on the critical path, in one launch: CTAs 0..7 build the diagonal
+// block's inverses, the others permute the right band (32 columns each) and fill a12t.
+__global__ void __launch_bounds__(256) lpp_post_kernel(float* __restrict__ a, int64_t lda, int n, int j0, int j1,
+                                                       int T, const int* __restrict__ plocal, float* __restrict__ a12t,
+                                                       int* __restrict__ perm, float* __restrict__ linv,
+                                                       float* __restrict__ uinvt, float* __restrict__ dblk) {
+  extern __shared__ float sm[];
+  if (blockIdx.x < 8) lpp_inverse_block(sm, blockIdx.x, a, lda, j0, j1 - j0, linv, uinvt, dblk);
+  else lpp_apply_band(sm, blockIdx.x - 8, a, lda, n, j0, j1, T, plocal, a12t, perm, true);
 }
 
 __global__ void iota32_kernel(int* p, int64_t n) {
@@ -403,15 +471,21 @@ __global__ void iota32_kernel(int* p, int64_t n) {
     p[i] = (int)i;
 }
 
-// The side stream and the two events of the look-ahead; released when the factorization returns
-// (work still queued on the side stream completes first).
+// SMs the look-ahead leaves free of the trailing update: the panel's and the inverses' CTAs
+constexpr int kLookAheadSms = 8;
+
+// The streams and events of the look-ahead; released when the factorization returns (work
+// still queued on the other streams completes first).
 struct LookAhead {
-  cudaStream_t side = nullptr;
-  cudaEvent_t next_done = nullptr, rest_done = nullptr;
+  cudaStream_t side = nullptr, aux = nullptr;
+  cudaEvent_t next_done = nullptr, rest_done = nullptr, panel_done = nullptr, left_done = nullptr;
   int open() {
     RM_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    RM_CUDA_TRY(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
     RM_CUDA_TRY(cudaEventCreateWithFlags(&next_done, cudaEventDisableTiming));
     RM_CUDA_TRY(cudaEventCreateWithFlags(&rest_done, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&panel_done, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&left_done, cudaEventDisableTiming));
     // rest_done starts out complete, so the first wait on it passes
     RM_CUDA_TRY(cudaEventRecord(rest_done, side));
     return RM_OK;
@@ -419,13 +493,17 @@ struct LookAhead {
   ~LookAhead() {
     if (next_done) cudaEventDestroy(next_done);
     if (rest_done) cudaEventDestroy(rest_done);
+    if (panel_done) cudaEventDestroy(panel_done);
+    if (left_done) cudaEventDestroy(left_done);
     if (side) cudaStreamDestroy(side);
+    if (aux) cudaStreamDestroy(aux);
   }
 };
 
 size_t getrf_lpp_f32_scratch_bytes(int64_t n) {
-  return (2 * (size_t)kLppCols * kLppCols + 2 * (size_t)n * kLppCols) * sizeof(float) + kLppRows * sizeof(int) +
-         2048;
+  // linv, uinvt, a12t, u12t; each panel's row permutation (256 ints per panel)
+  return (2 * (size_t)kLppCols * kLppCols + 2 * (size_t)n * kLppCols) * sizeof(float) +
+         (size_t)((n + kLppCols - 1) / kLppCols) * kLppRows * sizeof(int) + 2048;
 }
 
 int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, unsigned* status, cudaStream_t stream,
@@ -440,15 +518,18 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
   static bool set = false;
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(lpp_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLppSmem));
+    RM_CUDA_TRY(cudaFuncSetAttribute(lpp_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
     set = true;
   }
   iota32_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 1024), 256, 0, stream>>>(perm, n);
   RM_LAUNCHED();
   // Look-ahead: the next panel's 128 columns of each trailing update go first, on `stream`;
-  // the rest of the update runs on a side stream on all SMs but one while the next panel
-  // (one CTA) factors on the SM left free; the panel's row permutation then waits for it.
+  // the rest of the update runs on a side stream on all SMs but 8 while the next panel (one
+  // CTA) factors on the SMs left free. After a panel, one launch builds its inverses (8 CTAs)
+  // and permutes the columns to the right of it, while a third stream permutes the columns to
+  // its left, which nothing reads again during the factorization.
   LookAhead la;
-  const bool ahead = n >= 1024 && device_sm_count() > 1;
+  const bool ahead = n >= 1024 && device_sm_count() > 2 * kLookAheadSms;
   if (ahead) RM_TRY(la.open());
   const int ni = (int)n;
   for (int J0 = 0; J0 < ni; J0 += kLppCols) {
@@ -457,11 +538,25 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
     const int J1 = J0 + nb;
     const int rest = ni - J1;
     float* dblk = dinv ? dinv + (size_t)(J0 / kLppCols) * kDiagMats * kLppCols * kLppCols : nullptr;
-    lpp_panel_kernel<<<1, kLppThreads, kLppSmem, stream>>>(a, lda, J0, nb, T, linv, uinvt, plocal, dblk, status);
+    int* pl = plocal + (size_t)(J0 / kLppCols) * kLppRows;
+    lpp_panel_kernel<<<1, kLppThreads, kLppSmem, stream>>>(a, lda, J0, nb, T, pl, status);
     RM_LAUNCHED();
+    const int left_chunks = (J0 + kApplyCols - 1) / kApplyCols, right_chunks = (rest + kApplyCols - 1) / kApplyCols;
+    // the left band: on the third stream once the panel is done (in stream order without look-ahead)
+    cudaStream_t left_stream = stream;
+    if (ahead) {
+      RM_CUDA_TRY(cudaEventRecord(la.panel_done, stream));
+      RM_CUDA_TRY(cudaStreamWaitEvent(la.aux, la.panel_done, 0));
+      left_stream = la.aux;
+    }
+    if (left_chunks > 0) {
+      lpp_apply_kernel<<<left_chunks, 256, kApplySmem, left_stream>>>(a, lda, ni, J0, J1, T, pl);
+      RM_LAUNCHED();
+    }
+    // the inverses and the right band, after the trailing update that writes the right band
     if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
-    const int chunks = (J0 + kApplyCols - 1) / kApplyCols + (rest + kApplyCols - 1) / kApplyCols;
-    lpp_apply_kernel<<<std::max(chunks, 1), 256, 0, stream>>>(a, lda, ni, J0, J1, T, plocal, a12t, perm);
+    lpp_post_kernel<<<8 + std::max(right_chunks, 1), 256, kInvSmem, stream>>>(a, lda, ni, J0, J1, T, pl, a12t, perm,
+                                                                               linv, uinvt, dblk);
     RM_LAUNCHED();
     if (rest == 0) break;
     float* a12 = a + (int64_t)J0 * lda + J1;
@@ -487,11 +582,15 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
       RM_CUDA_TRY(cudaEventRecord(la.next_done, stream));
       RM_CUDA_TRY(cudaStreamWaitEvent(la.side, la.next_done, 0));
       RM_TRY(sgemm_tc(3, rest, rest - nn, nb, -1.0f, l21, lda, u12t + (size_t)nn * kLppCols, kLppCols, 1.0f, a22 + nn,
-                      lda, status, la.side, nullptr, 0, device_sm_count() - 1));
+                      lda, status, la.side, nullptr, 0, device_sm_count() - kLookAheadSms));
       RM_CUDA_TRY(cudaEventRecord(la.rest_done, la.side));
     }
   }
-  if (ahead) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
+  if (ahead) {
+    RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
+    RM_CUDA_TRY(cudaEventRecord(la.left_done, la.aux));  // the last left band
+    RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.left_done, 0));
+  }
   return RM_OK;
 }
 
