@@ -26,8 +26,8 @@
 //                      a buffer, and the global permutation
 //   lpp_apply_kernel : the permutation of the columns left of the panel (off the critical
 //                      path: nothing reads them again during the factorization)
-//   sgemm_tc         : U12^T = A12^T (L11^-1)^T, written both to a buffer and over A12
-//   sgemm_tc         : L21 = A21 U11^-1 for the rows below the panel, in place
+//   sgemm_tc_pair    : U12^T = A12^T (L11^-1)^T, written both to a buffer and over A12, and
+//                      L21 = A21 U11^-1 for the rows below the panel, in place (one launch)
 //   sgemm_tc         : A22 -= L21 U12
 // All products are 3xTF32 (float32-level) on tcgen05 with TMEM accumulators.
 #include <climits>
@@ -559,16 +559,14 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
                                                                                linv, uinvt, dblk);
     RM_LAUNCHED();
     if (rest == 0) break;
-    float* a12 = a + (int64_t)J0 * lda + J1;
-    // U12^T = A12^T (L11^-1)^T, also written transposed over A12
-    RM_TRY(sgemm_tc(3, rest, nb, nb, 1.0f, a12t, kLppCols, linv, kLppCols, 0.0f, u12t, kLppCols, status, stream, a12,
-                    lda));
+    // in one launch: U12^T = A12^T (L11^-1)^T, also written transposed over A12, and
     // L21 = A21 U11^-1 for the rows below the panel (the panel's own rows are done), in place
+    float* a12 = a + (int64_t)J0 * lda + J1;
     const int below = ni - (J0 + T);
-    if (below > 0) {
-      float* a21b = a + (int64_t)(J0 + T) * lda + J0;
-      RM_TRY(sgemm_tc(3, below, nb, nb, 1.0f, a21b, lda, uinvt, kLppCols, 0.0f, a21b, lda, status, stream));
-    }
+    float* a21b = a + (int64_t)(J0 + T) * lda + J0;
+    const SgemmOperands u12{rest, a12t, kLppCols, linv, kLppCols, u12t, kLppCols, a12, lda};
+    const SgemmOperands l21b{std::max(below, 0), a21b, lda, uinvt, kLppCols, a21b, lda, nullptr, 0};
+    RM_TRY(sgemm_tc_pair(3, u12, l21b, nb, nb, 1.0f, 0.0f, status, stream));
     // A22 -= L21 U12: the next panel's columns, then the rest
     const float* l21 = a + (int64_t)J1 * lda + J0;
     float* a22 = a + (int64_t)J1 * lda + J1;

@@ -24,6 +24,21 @@ int scale_device(double* c, int64_t ldc, int64_t m, int64_t n, double beta, cuda
 int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* b,
              int64_t ldb, float beta, float* c, int64_t ldc, unsigned* status, cudaStream_t stream,
              float* ct = nullptr, int64_t ldct = 0, int max_ctas = 0);
+// Two products C = alpha A B^T + beta C with the same n, k, alpha and beta in one persistent
+// launch (the first's output tiles first); a product with m == 0 is skipped.
+struct SgemmOperands {
+  int64_t m;
+  const float* a;
+  int64_t lda;
+  const float* b;
+  int64_t ldb;
+  float* c;
+  int64_t ldc;
+  float* ct;  // optional transposed copy of C (beta == 0 only through the TMA epilogue)
+  int64_t ldct;
+};
+int sgemm_tc_pair(int passes, const SgemmOperands& x, const SgemmOperands& y, int64_t n, int64_t k, float alpha,
+                  float beta, unsigned* status, cudaStream_t stream, int max_ctas = 0);
 int transpose_f32(const float* src, int64_t lds, int64_t m, int64_t n, float* dst, int64_t ldd, cudaStream_t stream);
 int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStream_t stream);
 int split_lo_f32(const float* x, int64_t ldx, int64_t m, int64_t k, float* lo, int64_t ldl, cudaStream_t stream);

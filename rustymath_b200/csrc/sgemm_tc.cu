@@ -66,11 +66,23 @@ __device__ __forceinline__ uint32_t lo_bits(uint32_t x) {
 
 }  // namespace tc
 
+// One of the (up to) two products of a launch: they share n, k, alpha and beta; the output
+// tiles of the first come first.
+struct SgemmPart {
+  float* c;
+  int64_t ldc;
+  float* ct;
+  int64_t ldct;
+  int m;
+  int tiles;
+};
+
 template <int PASSES, bool TMA_EPI>
 __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
     sgemm_tc_kernel(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
-                    const __grid_constant__ CUtensorMap tm_c, float* __restrict__ c, int64_t ldc,
-                    float* __restrict__ ct, int64_t ldct, int m, int n, int k, float alpha, float beta,
+                    const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_a2,
+                    const __grid_constant__ CUtensorMap tm_b2, const __grid_constant__ CUtensorMap tm_c2,
+                    const SgemmPart p1, const SgemmPart p2, int n, int k, float alpha, float beta,
                     unsigned* status) {
   using namespace tc;
   using C = Cfg<PASSES>;
@@ -90,8 +102,14 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntn = (n + BN - 1) / BN;
-  const int tiles = ((m + BM - 1) / BM) * ntn;
+  const int tiles = p1.tiles + p2.tiles;
   const int ktiles = (k + BK - 1) / BK;
+  // tile -> (its product, its index within it)
+  auto part = [&](int tile, int& lt) -> const SgemmPart& {
+    const bool second = tile >= p1.tiles;
+    lt = second ? tile - p1.tiles : tile;
+    return second ? p2 : p1;
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -122,10 +140,19 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
     if (lane == 0) {
       tma_prefetch_desc(&tm_a);
       tma_prefetch_desc(&tm_b);
+      if (p2.tiles > 0) {
+        tma_prefetch_desc(&tm_a2);
+        tma_prefetch_desc(&tm_b2);
+      }
       int it = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+        int ltile;
+        part(tile, ltile);
+        const bool second = tile >= p1.tiles;
+        const CUtensorMap* ma = second ? &tm_a2 : &tm_a;
+        const CUtensorMap* mb = second ? &tm_b2 : &tm_b;
+        const int m0 = (ltile / ntn) * BM, n0 = (ltile % ntn) * BN;
         for (int kt = 0; kt < ktiles; ++kt, ++it) {
           const int s = it % S;
           if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, status)) {
@@ -134,8 +161,8 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
           }
           uint8_t* st = smem + s * C::STAGE_BYTES;
           mbar_arrive_expect_tx(&full[s], LOAD_BYTES);
-          tma_load_2d(st, &tm_a, &full[s], kt * BK, m0);
-          tma_load_2d(st + TILE_BYTES, &tm_b, &full[s], kt * BK, n0);
+          tma_load_2d(st, ma, &full[s], kt * BK, m0);
+          tma_load_2d(st + TILE_BYTES, mb, &full[s], kt * BK, n0);
         }
       }
       // the copies still in flight land before this thread leaves (bounded)
@@ -196,8 +223,11 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
       if (lane == 0) {
         tc::bulk_wait_read<0>();  // the store that last used this buffer has read it
         const int b = ci & 1;
+        int lt2;
+        part(tile, lt2);
         mbar_arrive_expect_tx(&cl[b], EPI_BUF);
-        tma_load_2d(ebuf + b * EPI_BUF, &tm_c, &cl[b], (tile % ntn) * BN + cb, (tile / ntn) * BM + q * 32);
+        tma_load_2d(ebuf + b * EPI_BUF, tile >= p1.tiles ? &tm_c2 : &tm_c, &cl[b], (lt2 % ntn) * BN + cb,
+                    (lt2 / ntn) * BM + q * 32);
       }
       __syncwarp();
     };
@@ -208,7 +238,13 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
       const int buf = lt & 1;
       if (!mbar_wait(&tfull[buf], (lt >> 1) & 1u, status)) break;
       tc::fence_after();
-      const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+      int ltile;
+      const SgemmPart& P = part(tile, ltile);
+      const CUtensorMap* mc = tile >= p1.tiles ? &tm_c2 : &tm_c;
+      float* const ct = P.ct;
+      const int64_t ldct = P.ldct;
+      const int m = P.m;
+      const int m0 = (ltile / ntn) * BM, n0 = (ltile % ntn) * BN;
       const int row0 = m0 + q * 32;
 #pragma unroll 1
       for (int cb = 0; cb < BN; cb += 32, ++ci) {
@@ -256,7 +292,7 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
         fence_proxy_async();  // the TMA store reads these through the async proxy
         __syncwarp();
         if (lane == 0) {
-          tc::tma_store_2d(&tm_c, eb, n0 + cb, row0);
+          tc::tma_store_2d(mc, eb, n0 + cb, row0);
           tc::bulk_commit();
         }
         // the next chunk of C (this tile's, or the next tile's first)
@@ -275,7 +311,14 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
       const int buf = lt & 1;
       if (!mbar_wait(&tfull[buf], (lt >> 1) & 1u, status)) break;
       tc::fence_after();
-      const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+      int ltile;
+      const SgemmPart& P = part(tile, ltile);
+      float* const c = P.c;
+      const int64_t ldc = P.ldc;
+      float* const ct = P.ct;
+      const int64_t ldct = P.ldct;
+      const int m = P.m;
+      const int m0 = (ltile / ntn) * BM, n0 = (ltile % ntn) * BN;
       const int row0 = m0 + q * 32;
 #pragma unroll 1
       for (int cb = 0; cb < BN; cb += 32) {
@@ -388,9 +431,8 @@ int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStrea
 }
 
 template <int PASSES, bool TMA_EPI>
-static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tcm, float* c, int64_t ldc,
-                        float* ct, int64_t ldct, int m, int n, int k, float alpha, float beta, unsigned* status,
-                        cudaStream_t stream, int max_ctas) {
+static int launch_sgemm(const CUtensorMap* maps, const SgemmPart& p1, const SgemmPart& p2, int n, int k, float alpha,
+                        float beta, unsigned* status, cudaStream_t stream, int max_ctas) {
   using C = tc::Cfg<PASSES>;
   static bool set = false;
   if (!set) {
@@ -398,37 +440,72 @@ static int launch_sgemm(const CUtensorMap& ta, const CUtensorMap& tb, const CUte
                                      (int)C::SMEM));
     set = true;
   }
-  const int64_t tiles = (int64_t)((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN);
+  const int64_t tiles = (int64_t)p1.tiles + p2.tiles;
   const int ctas = max_ctas > 0 ? std::min(max_ctas, device_sm_count()) : device_sm_count();
   const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctas);
-  sgemm_tc_kernel<PASSES, TMA_EPI><<<grid, C::THREADS, C::SMEM, stream>>>(ta, tb, tcm, c, ldc, ct, ldct, m, n, k,
-                                                                          alpha, beta, status);
+  sgemm_tc_kernel<PASSES, TMA_EPI><<<grid, C::THREADS, C::SMEM, stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4],
+                                                                          maps[5], p1, p2, n, k, alpha, beta, status);
   RM_LAUNCHED();
   return RM_OK;
+}
+
+namespace {
+// The tensor maps of one product (A, B and, for the TMA epilogue, C) and its tile count.
+int prepare_part(const SgemmOperands& o, int64_t n, int64_t k, bool tma_epi, CUtensorMap* maps, SgemmPart* part) {
+  if (o.m > INT32_MAX) return RM_BAD_ARG;
+  RM_TRY(make_tensor_map_2d(&maps[0], o.a, 4, k, o.m, o.lda * 4, tc::BK, tc::BM, true));
+  RM_TRY(make_tensor_map_2d(&maps[1], o.b, 4, k, n, o.ldb * 4, tc::BK, tc::BN, true));
+  if (tma_epi) RM_TRY(make_tensor_map_2d(&maps[2], o.c, 4, n, o.m, o.ldc * 4, 32, 32, true));
+  else memset(&maps[2], 0, sizeof maps[2]);
+  *part = {o.c, o.ldc, o.ct, o.ldct, (int)o.m, (int)(((o.m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN))};
+  return RM_OK;
+}
+
+// C through TMA when its base and row stride are 16-byte aligned (the transposed copy,
+// written directly, only beside beta == 0)
+bool tma_epilogue_ok(const SgemmOperands& o, float beta) {
+  return (reinterpret_cast<uintptr_t>(o.c) & 15) == 0 && (o.ldc * 4) % 16 == 0 && !(o.ct && beta != 0.0f);
+}
+}  // namespace
+
+int sgemm_tc_pair(int passes, const SgemmOperands& x, const SgemmOperands& y, int64_t n, int64_t k, float alpha,
+                  float beta, unsigned* status, cudaStream_t stream, int max_ctas) {
+  if (passes != 1 && passes != 3) return RM_BAD_ARG;
+  if (n > INT32_MAX || k > INT32_MAX || k == 0) return RM_BAD_ARG;
+  if (n == 0) return RM_OK;
+  const SgemmOperands* live[2];
+  int cnt = 0;
+  if (x.m > 0) live[cnt++] = &x;
+  if (y.m > 0) live[cnt++] = &y;
+  if (cnt == 0) return RM_OK;
+  const bool tma_epi = tma_epilogue_ok(*live[0], beta) && (cnt == 1 || tma_epilogue_ok(*live[1], beta));
+  CUtensorMap maps[6];
+  SgemmPart p[2];
+  RM_TRY(prepare_part(*live[0], n, k, tma_epi, maps, &p[0]));
+  if (cnt == 2) {
+    RM_TRY(prepare_part(*live[1], n, k, tma_epi, maps + 3, &p[1]));
+  } else {
+    memcpy(maps + 3, maps, 3 * sizeof(CUtensorMap));
+    p[1] = {nullptr, 0, nullptr, 0, 0, 0};
+  }
+  const int ni = (int)n, ki = (int)k;
+  if (passes == 3)
+    return tma_epi ? launch_sgemm<3, true>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas)
+                   : launch_sgemm<3, false>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas);
+  return tma_epi ? launch_sgemm<1, true>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas)
+                 : launch_sgemm<1, false>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas);
 }
 
 int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* b,
              int64_t ldb, float beta, float* c, int64_t ldc, unsigned* status, cudaStream_t stream, float* ct,
              int64_t ldct, int max_ctas) {
   if (m == 0 || n == 0) return RM_OK;
-  if (passes != 1 && passes != 3) return RM_BAD_ARG;
-  if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || k == 0) return RM_BAD_ARG;
-  CUtensorMap ta, tb;
-  RM_TRY(make_tensor_map_2d(&ta, a, 4, k, m, lda * 4, tc::BK, tc::BM, true));
-  RM_TRY(make_tensor_map_2d(&tb, b, 4, k, n, ldb * 4, tc::BK, tc::BN, true));
-  // C through TMA when its base and row stride are 16-byte aligned (the transposed copy,
-  // written directly, only beside beta == 0)
-  CUtensorMap tcm;
-  const bool tma_epi = (reinterpret_cast<uintptr_t>(c) & 15) == 0 && (ldc * 4) % 16 == 0 && !(ct && beta != 0.0f);
-  if (tma_epi) RM_TRY(make_tensor_map_2d(&tcm, c, 4, n, m, ldc * 4, 32, 32, true));
-  else memset(&tcm, 0, sizeof tcm);
-  const int mi = (int)m, ni = (int)n, ki = (int)k;
-  if (passes == 3)
-    return tma_epi ? launch_sgemm<3, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas)
-                   : launch_sgemm<3, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas);
-  return tma_epi ? launch_sgemm<1, true>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas)
-                 : launch_sgemm<1, false>(ta, tb, tcm, c, ldc, ct, ldct, mi, ni, ki, alpha, beta, status, stream, max_ctas);
+  if (m > INT32_MAX) return RM_BAD_ARG;
+  const SgemmOperands x{m, a, lda, b, ldb, c, ldc, ct, ldct};
+  const SgemmOperands none{0, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0};
+  return sgemm_tc_pair(passes, x, none, n, k, alpha, beta, status, stream, max_ctas);
 }
+
 
 // dst (n x m, ldd) = src^T for the m x n row-major float32 src (lds): 32x32 tiles through
 // shared memory, both sides coalesced.
