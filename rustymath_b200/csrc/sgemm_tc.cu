@@ -14,9 +14,10 @@
 // 128 x 128 FP32 accumulators) and its lane 0 issues the MMAs (M=128, N=128, K=8 per
 // instruction), alternating accumulators between tiles so that the next tile's MMAs run
 // while the epilogue drains the last one; warps 2..5 are the epilogue (one 32-lane TMEM
-// quarter each), in 32 x 32 chunks: C's chunk comes in by TMA one chunk ahead (when beta is
-// not zero), alpha*acc + beta*C is formed in the same swizzled shared-memory buffer and goes
-// out as an asynchronous TMA store, so no global access stalls these warps; the optional
+// quarter each), in 32 x 32 chunks through six buffers per warp: C's chunks come in by TMA
+// five chunks ahead (when beta is not zero), alpha*acc + beta*C is formed in the same
+// swizzled shared-memory buffer and goes out as an asynchronous TMA store, so no global
+// access stalls these warps; the optional
 // transposed copy is written from registers in coalesced columns. (When C's address or row
 // stride does not suit TMA, the epilogue stages through shared memory and writes coalesced
 // rows itself.) For three passes warps 6..9 form the low parts of each stage. Every wait is
@@ -33,12 +34,13 @@ constexpr int TILE_BYTES = BM * BK * 4;     // 16 KB per operand tile (BM == BN)
 constexpr uint32_t TMEM_COLS = 256;         // two accumulators of BN columns
 constexpr int STG_STRIDE = 33;              // direct epilogue: 32 x 32 floats per warp, padded
 constexpr int EPI_BUF = 32 * 32 * 4;        // TMA epilogue: one 32 x 32 chunk, 128-byte swizzle
-constexpr int STG_BYTES = 4 * 2 * EPI_BUF;  // two chunk buffers per epilogue warp (>= the direct staging)
+constexpr int EPI_NBUF = 6;                 // chunk buffers per epilogue warp: C is read 5 chunks ahead
+constexpr int STG_BYTES = 4 * EPI_NBUF * EPI_BUF;  // (>= the direct epilogue's staging)
 
 template <int PASSES>
 struct Cfg {
   static constexpr int OPS = PASSES == 3 ? 4 : 2;  // tiles per stage: A, B, (A_lo, B_lo)
-  static constexpr int STAGES = PASSES == 3 ? 3 : 6;
+  static constexpr int STAGES = PASSES == 3 ? 2 : 4;
   static constexpr int STAGE_BYTES = OPS * TILE_BYTES;
   static constexpr int LO_WARPS = PASSES == 3 ? 4 : 0;
   static constexpr int THREADS = 32 * (6 + LO_WARPS);
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
   uint64_t* tempty = tfull + 2;     // the epilogue has read an accumulator out
   uint64_t* mma_done = tempty + 2;  // every MMA issued has completed
   uint64_t* cload = mma_done + 1;   // [epilogue warp][buffer]: a chunk of C has landed
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + 8);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cload + 4 * EPI_NBUF);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntn = (n + BN - 1) / BN;
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
       mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
     }
     mbar_init(mma_done, 1);
-    for (int b = 0; b < 8; ++b) mbar_init(&cload[b], 1);
+    for (int b = 0; b < 4 * EPI_NBUF; ++b) mbar_init(&cload[b], 1);
     fence_barrier_init();
   }
   if (warp == 1) {
@@ -214,26 +216,37 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
   } else if (warp < 6 && TMA_EPI) {
     // ---------------- epilogue through TMA: warps 2..5, TMEM lane quarter warp % 4
     const int q = warp & 3, ew = warp - 2;
-    uint8_t* ebuf = reinterpret_cast<uint8_t*>(stg_all) + ew * 2 * EPI_BUF;
-    uint64_t* cl = cload + 2 * ew;
+    uint8_t* ebuf = reinterpret_cast<uint8_t*>(stg_all) + ew * EPI_NBUF * EPI_BUF;
+    uint64_t* cl = cload + EPI_NBUF * ew;
     const bool load_c = beta != 0.0f;
-    // chunk ci (counted over this CTA's tiles) uses buffer ci & 1
-    auto prefetch = [&](int ci, int tile, int cb) {
-      if (!load_c || tile >= tiles) return;
-      if (lane == 0) {
-        tc::bulk_wait_read<0>();  // the store that last used this buffer has read it
-        const int b = ci & 1;
-        int lt2;
-        part(tile, lt2);
-        mbar_arrive_expect_tx(&cl[b], EPI_BUF);
-        tma_load_2d(ebuf + b * EPI_BUF, tile >= p1.tiles ? &tm_c2 : &tm_c, &cl[b], (lt2 % ntn) * BN + cb,
-                    (lt2 / ntn) * BM + q * 32);
+    // Chunk ci (counted over this CTA's tiles, BN / 32 per tile) uses buffer ci % EPI_NBUF, and
+    // C's chunks are loaded EPI_NBUF - 1 ahead of the one being formed.
+    constexpr int CPT = BN / 32;
+    const int my_tiles = (int)blockIdx.x < tiles ? (tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    const int chunks = my_tiles * CPT;
+    int issued = 0;  // chunks of C whose load has been issued
+    // Issues the loads of chunks issued..upto-1. Called once a chunk's store is committed (or
+    // before the first), so a buffer's previous store is at most one group back.
+    auto prefetch_to = [&](int upto) {
+      if (!load_c) return;
+      upto = min(upto, chunks);
+      for (; issued < upto; ++issued) {
+        if (lane == 0) {
+          tc::bulk_wait_read<1>();  // the store that last used this buffer has read it
+          const int b = issued % EPI_NBUF;
+          const int tile = (int)blockIdx.x + (issued / CPT) * (int)gridDim.x, cb = (issued % CPT) * 32;
+          int lt2;
+          part(tile, lt2);
+          mbar_arrive_expect_tx(&cl[b], EPI_BUF);
+          tma_load_2d(ebuf + b * EPI_BUF, tile >= p1.tiles ? &tm_c2 : &tm_c, &cl[b], (lt2 % ntn) * BN + cb,
+                      (lt2 / ntn) * BM + q * 32);
+        }
       }
       __syncwarp();
     };
     int lt = 0, ci = 0;
     bool ok = true;
-    prefetch(0, blockIdx.x, 0);
+    prefetch_to(EPI_NBUF - 1);
     for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++lt) {
       const int buf = lt & 1;
       if (!mbar_wait(&tfull[buf], (lt >> 1) & 1u, status)) break;
@@ -255,15 +268,15 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(&tempty[buf]);
         }
-        const int b = ci & 1;
+        const int b = ci % EPI_NBUF;
         uint8_t* eb = ebuf + b * EPI_BUF;
         if (load_c) {
-          if (!mbar_wait(&cl[b], (ci >> 1) & 1u, status)) {
+          if (!mbar_wait(&cl[b], (ci / EPI_NBUF) & 1u, status)) {
             ok = false;
             break;
           }
         } else {
-          if (lane == 0) tc::bulk_wait_read<1>();  // the store two chunks back has read this buffer
+          if (lane == 0) tc::bulk_wait_read<EPI_NBUF - 1>();  // the store EPI_NBUF chunks back has read this buffer
           __syncwarp();
         }
         // this lane's row of the chunk: alpha * acc + beta * C, in place
@@ -295,11 +308,11 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
           tc::tma_store_2d(mc, eb, n0 + cb, row0);
           tc::bulk_commit();
         }
-        // the next chunk of C (this tile's, or the next tile's first)
-        if (cb + 32 < BN) prefetch(ci + 1, tile, cb + 32);
-        else prefetch(ci + 1, tile + gridDim.x, 0);
+        prefetch_to(ci + EPI_NBUF);  // C's chunk EPI_NBUF - 1 ahead of the next
       }
     }
+    // loads of C still in flight (only after a wait gave up) land before the CTA ends (bounded)
+    for (int j = ci; j < issued; ++j) mbar_wait(&cl[j % EPI_NBUF], (j / EPI_NBUF) & 1u, status);
     if (lane == 0) tc::bulk_wait_all();  // every store has landed before the CTA ends
     __syncwarp();
   } else if (warp < 6) {
