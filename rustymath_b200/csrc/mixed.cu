@@ -111,29 +111,17 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
   const int r = tid;
   float* blk = a + (int64_t)j0 * lda + j0;
   if (nb == kLppCols) {
-    // a warp per row, a 16-byte load per lane, eight rows in flight; lane q stores its four
-    // floats rotated by q / 8 so that the stores of a warp hit 32 distinct banks
+    // asynchronous 4-byte copies, every one of a thread's in flight at once: a warp per row,
+    // lane l the row's floats 4l..4l+3 (each warp reads 512 contiguous bytes per row), in an
+    // order rotated by l / 8 so that the shared-memory writes of a warp hit 32 distinct banks
     const int rot = lane >> 3;
-    for (int r0 = warp; r0 < T; r0 += 8 * (kLppThreads / 32)) {
-      float4 v[8];
+    for (int rr = warp; rr < T; rr += kLppThreads / 32)
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int rr = r0 + u * (kLppThreads / 32);
-        v[u] = rr < T ? *reinterpret_cast<const float4*>(blk + (int64_t)rr * lda + 4 * lane) : make_float4(0, 0, 0, 0);
+      for (int t = 0; t < 4; ++t) {
+        const int c = 4 * lane + ((t + rot) & 3);
+        cp_async4(&P[rr][c], blk + (int64_t)rr * lda + c);
       }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int rr = r0 + u * (kLppThreads / 32);
-        if (rr < T) {
-          const float e[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const int q = (t + rot) & 3;
-            P[rr][4 * lane + q] = q == 0 ? e[0] : q == 1 ? e[1] : q == 2 ? e[2] : e[3];
-          }
-        }
-      }
-    }
+    cp_async_wait_all();
   } else {
     for (int e = tid; e < T * nb; e += kLppThreads) {
       const int rr = e / nb, c = e % nb;
@@ -300,29 +288,16 @@ __device__ __forceinline__ void lpp_inverse_block(float* sm, int bid, const floa
   const float* blk = a + (int64_t)j0 * lda + j0;
   // M from row a0 on: a warp per stored row, lanes along it
   if (nb == kLppCols) {
-    // a 16-byte load per lane, all of a thread's rows in flight; lane l stores its four floats
-    // rotated by l / 8, so that the stores of a warp hit 32 distinct banks
+    // asynchronous 4-byte copies, all in flight at once; lane l copies floats 4l..4l+3 of a row
+    // in an order rotated by l / 8, so that the shared-memory writes of a warp hit distinct banks
     const int rot = lane >> 3;
-    float4 v[16];
+    for (int i = a0 + warp; i < kLppCols; i += 8)
 #pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int i = a0 + warp + 8 * u;
-      v[u] = i < kLppCols ? *reinterpret_cast<const float4*>(blk + (int64_t)i * lda + 4 * lane) : make_float4(0, 0, 0, 0);
-    }
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const int i = a0 + warp + 8 * u;
-      if (i < kLppCols) {
-        const float e[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int q = (t + rot) & 3;
-          const float x = q == 0 ? e[0] : q == 1 ? e[1] : q == 2 ? e[2] : e[3];
-          if (m == 0) M[i][4 * lane + q] = x;
-          else M[4 * lane + q][i] = x;
-        }
+      for (int t = 0; t < 4; ++t) {
+        const int k = 4 * lane + ((t + rot) & 3);
+        cp_async4(m == 0 ? &M[i][k] : &M[k][i], blk + (int64_t)i * lda + k);
       }
-    }
+    cp_async_wait_all();
   } else {
     for (int i = a0 + warp; i < kLppCols; i += 8)
       for (int k = a0 + lane; k < kLppCols; k += 32) {

@@ -111,6 +111,12 @@ __device__ __forceinline__ uint32_t swz128_f32(uint32_t row, uint32_t col) {
 // ------------------------------------------------------------------ warp helpers
 __device__ __forceinline__ bool elect_one() { return (threadIdx.x & 31) == 0; }
 
+// 4-byte asynchronous copy global -> shared (no register staging; completes at cp_async_wait_all)
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 }  // namespace rm
 
 // ------------------------------------------------------------------ host helpers
