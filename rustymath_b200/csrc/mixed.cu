@@ -29,7 +29,9 @@
 //   sgemm_tc_pair    : U12^T = A12^T (L11^-1)^T, written both to a buffer and over A12, and
 //                      L21 = A21 U11^-1 for the rows below the panel, in place (one launch)
 //   sgemm_tc         : A22 -= L21 U12
-// All products are 3xTF32 (float32-level) on tcgen05 with TMEM accumulators.
+// All products are 3xTF32 (float32-level) on tcgen05 with TMEM accumulators. Along this chain
+// each kernel is a programmatic dependent of the one before it (its launch and set-up overlap
+// that kernel's end; it reads nothing of it before griddepcontrol.wait).
 #include <climits>
 
 #include "rm_internal.h"
@@ -110,6 +112,8 @@ __global__ void __launch_bounds__(kLppThreads, 1) lpp_panel_kernel(float* __rest
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r = tid;
   float* blk = a + (int64_t)j0 * lda + j0;
+  griddep_launch_dependents();
+  griddep_wait();  // the update of these columns has completed
   if (nb == kLppCols) {
     // asynchronous 4-byte copies, every one of a thread's in flight at once: a warp per row,
     // lane l the row's floats 4l..4l+3 (each warp reads 512 contiguous bytes per row), in an
@@ -437,6 +441,8 @@ __global__ void __launch_bounds__(256) lpp_post_kernel(float* __restrict__ a, in
                                                        int* __restrict__ perm, float* __restrict__ linv,
                                                        float* __restrict__ uinvt, float* __restrict__ dblk) {
   extern __shared__ float sm[];
+  griddep_launch_dependents();
+  griddep_wait();  // the panel has completed
   if (blockIdx.x < 8) lpp_inverse_block(sm, blockIdx.x, a, lda, j0, j1 - j0, linv, uinvt, dblk);
   else lpp_apply_band(sm, blockIdx.x - 8, a, lda, n, j0, j1, T, plocal, a12t, perm, true);
 }
@@ -514,7 +520,8 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
     const int rest = ni - J1;
     float* dblk = dinv ? dinv + (size_t)(J0 / kLppCols) * kDiagMats * kLppCols * kLppCols : nullptr;
     int* pl = plocal + (size_t)(J0 / kLppCols) * kLppRows;
-    lpp_panel_kernel<<<1, kLppThreads, kLppSmem, stream>>>(a, lda, J0, nb, T, pl, status);
+    RM_CUDA_TRY(launch_dependent(lpp_panel_kernel, dim3(1), dim3(kLppThreads), kLppSmem, stream, a, lda, J0, nb, T, pl,
+                                 status));
     RM_LAUNCHED();
     const int left_chunks = (J0 + kApplyCols - 1) / kApplyCols, right_chunks = (rest + kApplyCols - 1) / kApplyCols;
     // the left band: on the third stream once the panel is done (in stream order without look-ahead)
@@ -530,8 +537,8 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
     }
     // the inverses and the right band, after the trailing update that writes the right band
     if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
-    lpp_post_kernel<<<8 + std::max(right_chunks, 1), 256, kInvSmem, stream>>>(a, lda, ni, J0, J1, T, pl, a12t, perm,
-                                                                               linv, uinvt, dblk);
+    RM_CUDA_TRY(launch_dependent(lpp_post_kernel, dim3(8 + std::max(right_chunks, 1)), dim3(256), kInvSmem, stream, a, lda,
+                                 ni, J0, J1, T, (const int*)pl, a12t, perm, linv, uinvt, dblk));
     RM_LAUNCHED();
     if (rest == 0) break;
     // in one launch: U12^T = A12^T (L11^-1)^T, also written transposed over A12, and

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <utility>
 
 #include "../../include/rm_cuda.h"
 
@@ -23,6 +24,30 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;
 
 __device__ __forceinline__ void flag_error(unsigned* status, unsigned bits) {
   if (status) atomicOr(status, bits);
+}
+
+// ------------------------------------------------------------------ programmatic dependent launch
+// A kernel launched with launch_dependent() may start while the kernel before it in the stream
+// is still running: it does its set-up, then griddep_wait() returns once that kernel has
+// completed and its memory is visible (at once for an ordinary launch). A kernel lets the next
+// one start early with griddep_launch_dependents(); without it that happens at its end.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                                   Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // ------------------------------------------------------------------ mbarrier

@@ -21,7 +21,8 @@
 // transposed copy is written from registers in coalesced columns. (When C's address or row
 // stride does not suit TMA, the epilogue stages through shared memory and writes coalesced
 // rows itself.) For three passes warps 6..9 form the low parts of each stage. Every wait is
-// bounded; TMEM is freed on every path.
+// bounded; TMEM is freed on every path. Launched as a programmatic dependent: barrier set-up
+// and the TMEM allocation overlap the end of the kernel before it.
 #include "rm_internal.h"
 #include "rm_tcgen05.cuh"
 
@@ -136,6 +137,10 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = *tmem_slot;
+  // set-up done: the next kernel in the stream may start its own; then wait for the previous
+  // one's results (no wait without a programmatic launch)
+  griddep_launch_dependents();
+  griddep_wait();
 
   if (warp == 0) {
     // ---------------- TMA producer
@@ -456,8 +461,8 @@ static int launch_sgemm(const CUtensorMap* maps, const SgemmPart& p1, const Sgem
   const int64_t tiles = (int64_t)p1.tiles + p2.tiles;
   const int ctas = max_ctas > 0 ? std::min(max_ctas, device_sm_count()) : device_sm_count();
   const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctas);
-  sgemm_tc_kernel<PASSES, TMA_EPI><<<grid, C::THREADS, C::SMEM, stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4],
-                                                                          maps[5], p1, p2, n, k, alpha, beta, status);
+  RM_CUDA_TRY(launch_dependent(sgemm_tc_kernel<PASSES, TMA_EPI>, dim3(grid), dim3(C::THREADS), C::SMEM, stream, maps[0],
+                               maps[1], maps[2], maps[3], maps[4], maps[5], p1, p2, n, k, alpha, beta, status));
   RM_LAUNCHED();
   return RM_OK;
 }
