@@ -691,7 +691,7 @@ def main():
                     "achieved": gbs, "peak": peak_hbm(), "unit": "GB/s", "frac": gbs / peak_hbm(),
                     "peak_source": peak_hbm_source()[1],
                     "bytes_per_launch": bytes_upd, "launch_us": 1e6 * t_upd, "tf32_tflops": tf32_tflops,
-                    "traffic": 268.48e6 + 200.21e6,
+                    "traffic": 268.47e6 + 201.07e6,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch at full size "
                                       "(bench.py --workload update, the 4th launch)"}
         peak64 = gemm_peak_f64(torch, dev)
