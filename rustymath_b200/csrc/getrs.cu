@@ -399,6 +399,162 @@ static int launch_trsv(const T* w, int64_t ldw, int n, const T* dinv, T* x, int6
   return RM_OK;
 }
 
+// The float32 block-Jacobi-scaled chain (PRE, 128-row blocks, tensor-core products) with its
+// blocks of the scaled triangle brought into shared memory by asynchronous copies, two blocks
+// ahead of the one being applied (a ring of three): a step's own time is then its product, not
+// the load latency of its block. Otherwise as trsv_chain_kernel<float, LOWER, false, 128, true>:
+// x_b = D_b^-1 y_b - sum_j pre_bj x_j, each x_j subtracted as it is released, in solve order;
+// pre holds full zero-padded 128 x 128 blocks (ld a multiple of 128), so every copy is in bounds.
+template <bool LOWER>
+__global__ void __launch_bounds__(kTB32 * 4)
+    trsv_pre_ring_kernel(const float* __restrict__ pre, int64_t ldp, int n, const float* __restrict__ dinv, float* x,
+                         int64_t ldx, int kc, int* flags, int* counter, unsigned* status) {
+  constexpr int TB = kTB32, THREADS = TB * 4, LDS = TB + 4, RING = 3, XS = 24;
+  extern __shared__ __align__(16) uint8_t smraw[];
+  float(*ring)[TB][LDS] = reinterpret_cast<float(*)[TB][LDS]>(smraw);
+  float(*xs)[XS] = reinterpret_cast<float(*)[XS]>(smraw + (size_t)RING * TB * LDS * sizeof(float));
+  __shared__ int ticket;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (n + TB - 1) / TB;
+  if (tid == 0) ticket = atomicAdd(counter, 1);
+  __syncthreads();
+  const int t = ticket;
+  const int b = LOWER ? t : nblk - 1 - t;
+  const int r0 = b * TB, rows = min(TB, n - r0);
+  auto dep = [&](int s) { return LOWER ? s : nblk - 1 - s; };  // the s-th block solved
+  const int g = lane >> 2, tq = lane & 3;
+  const int fr = 16 * (warp >> 1) + g, fc = 8 * (warp & 1) + 2 * tq;
+  auto prow = [&](int i) { return fr + 8 * (i >> 1); };
+  auto pcol = [&](int i) { return fc + (i & 1); };
+
+  float acc[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = prow(i), c = pcol(i);
+    acc[i] = (r < rows && c < kc) ? x[(int64_t)(r0 + r) * ldx + c] : 0.0f;
+  }
+  // item 0 is D_b^-1, item i >= 1 the block (b, dep(i - 1)); an item past t commits an empty
+  // group, so that every thread counts the same groups
+  auto issue = [&](int it) {
+    if (it <= t) {
+      const float* src;
+      int64_t ld;
+      if (it == 0) {
+        src = dinv + ((int64_t)b * kDiagMats + (LOWER ? 0 : 1)) * TB * TB;
+        ld = TB;
+      } else {
+        src = pre + (int64_t)b * TB * ldp + (int64_t)dep(it - 1) * TB;
+        ld = ldp;
+      }
+      float(*dst)[LDS] = ring[it % RING];
+#pragma unroll
+      for (int q = 0; q < TB * TB / 4 / THREADS; ++q) {
+        const int e = tid + q * THREADS, r = e >> 5, c = (e & 31) * 4;
+        cp_async16(&dst[r][c], src + (int64_t)r * ld + c);
+      }
+    }
+    cp_async_commit();
+  };
+  // a += sign * blk xs (this thread's fragment), 3xTF32 on the tensor cores
+  auto apply = [&](const float(*blk)[LDS], float sign) {
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+    for (int k8 = 0; k8 < TB; k8 += 8) {
+      const float av[4] = {sign * blk[fr][k8 + tq], sign * blk[fr + 8][k8 + tq], sign * blk[fr][k8 + tq + 4],
+                           sign * blk[fr + 8][k8 + tq + 4]};
+      const float bv0 = xs[k8 + tq][8 * (warp & 1) + g], bv1 = xs[k8 + tq + 4][8 * (warp & 1) + g];
+      uint32_t ah[4], al[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        ah[i] = tc::to_tf32(av[i]);
+        al[i] = tc::to_tf32(av[i] - __uint_as_float(ah[i]));
+      }
+      const uint32_t bh0 = tc::to_tf32(bv0), bh1 = tc::to_tf32(bv1);
+      const uint32_t bl0 = tc::to_tf32(bv0 - __uint_as_float(bh0)), bl1 = tc::to_tf32(bv1 - __uint_as_float(bh1));
+      tc::mma_tf32_16x8x8(d, al, bh0, bh1);
+      tc::mma_tf32_16x8x8(d, ah, bl0, bl1);
+      tc::mma_tf32_16x8x8(d, ah, bh0, bh1);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[i] += d[i];
+  };
+  auto fetch = [&](int j) -> bool {  // wait for block j's release, then x_j into xs
+    bool seen = ld_acquire(&flags[j]) != 0;
+    if (!seen) {
+      const uint64_t start = global_ns();
+      while (!(seen = ld_acquire(&flags[j]) != 0)) {
+        if (global_ns() - start > kWaitLimitNs) break;
+      }
+    }
+    if (seen) {
+      const int c0 = j * TB, cols = min(TB, n - c0);
+      for (int e = tid; e < TB * kKC; e += THREADS) {
+        const int r = e / kKC, c = e % kKC;
+        xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : 0.0f;
+      }
+    }
+    if (!__syncthreads_and(seen ? 1 : 0)) {
+      if (tid == 0) flag_error(status, RM_DEV_TIMEOUT);
+      return false;
+    }
+    return true;
+  };
+
+  issue(0);
+  issue(1);
+  issue(2);
+  // z_b = D_b^-1 y_b
+#pragma unroll
+  for (int i = 0; i < 4; ++i) xs[prow(i)][pcol(i)] = acc[i];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) acc[i] = 0.0f;
+  cp_async_wait<2>();  // item 0 has landed
+  __syncthreads();
+  apply(ring[0], 1.0f);
+  bool ok = true;
+  for (int s = 0; s < t; ++s) {
+    const int it = s + 1;
+    __syncthreads();  // the last apply's reads of its slot and of xs are done
+    issue(it + 2);    // into the slot of item it - 1, applied already
+    if (!fetch(dep(s))) {
+      ok = false;
+      break;
+    }
+    cp_async_wait<2>();  // item it has landed (it + 1 and it + 2 may be in flight)
+    __syncthreads();
+    apply(ring[it % RING], -1.0f);
+  }
+  cp_async_wait_all();  // no copy into shared memory outlives the CTA
+  if (ok) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = prow(i), c = pcol(i);
+      if (r < rows && c < kc) x[(int64_t)(r0 + r) * ldx + c] = acc[i];
+    }
+  }
+  // every thread's x is written before the barrier; thread 0's release store, ordered after it,
+  // publishes them device-wide
+  __syncthreads();
+  if (tid == 0) st_release(&flags[b], 1);
+}
+
+template <bool LOWER>
+static int launch_trsv_pre_ring(const float* pre, int64_t ldp, int n, const float* dinv, float* x, int64_t ldx, int kc,
+                                int* flags, int* counter, unsigned* status, cudaStream_t stream) {
+  constexpr size_t smem = (size_t)3 * kTB32 * (kTB32 + 4) * sizeof(float) + (size_t)kTB32 * 24 * sizeof(float);
+  static bool set = false;
+  if (!set) {
+    RM_CUDA_TRY(cudaFuncSetAttribute(trsv_pre_ring_kernel<LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    set = true;
+  }
+  const int nblk = (n + kTB32 - 1) / kTB32;
+  trsv_pre_ring_kernel<LOWER><<<nblk, kTB32 * 4, smem, stream>>>(pre, ldp, n, dinv, x, ldx, kc, flags, counter,
+                                                                   status);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
 // Row permutation of an n x k row-major matrix: x[i] = b[perm[i]] (gather), or, with
 // SCATTER, x[perm[i]] = b[i]. perm == NULL copies. A position outside 0..n-1 (a caller's
 // perm) sets RM_DEV_BAD_INDEX and is skipped.
@@ -631,10 +787,9 @@ int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv
     int* f = flags + (size_t)ch * 2 * (nblk + 1);
     float* xc = x + ch * kKC;
     if (pre) {
-      RM_TRY((launch_trsv<float, true, false, kTB32, true>(pre, ldp, (int)n, dinv, xc, ldx, kc, f, f + nblk, status,
-                                                           stream)));
-      RM_TRY((launch_trsv<float, false, false, kTB32, true>(pre, ldp, (int)n, dinv, xc, ldx, kc, f + nblk + 1,
-                                                            f + 2 * nblk + 1, status, stream)));
+      RM_TRY(launch_trsv_pre_ring<true>(pre, ldp, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream));
+      RM_TRY(launch_trsv_pre_ring<false>(pre, ldp, (int)n, dinv, xc, ldx, kc, f + nblk + 1, f + 2 * nblk + 1, status,
+                                         stream));
     } else {
       RM_TRY((launch_trsv<float, true, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream)));
       RM_TRY((launch_trsv<float, false, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f + nblk + 1,
