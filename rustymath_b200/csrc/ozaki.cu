@@ -131,6 +131,19 @@ __global__ void split_cols_kernel(const double* __restrict__ b, int64_t ldb, int
   }
 }
 
+// Output tile t of a persistent walk -> (tile row, tile column), in bands of kBand tile rows:
+// down a band's rows first, then across its columns, so that the ~148 tiles in flight at once
+// read about kBand row panels of A's slices and 148 / kBand column panels of B's (some tens of
+// MB, resident in L2) instead of one row panel and 148 column panels.
+constexpr int kBand = 16;
+__device__ __forceinline__ void tile_coords(int t, int ntm, int ntn, int& tm, int& tn) {
+  const int per_band = kBand * ntn;
+  const int band = t / per_band, in = t - band * per_band;
+  const int rows = min(kBand, ntm - band * kBand);
+  tm = band * kBand + in % rows;
+  tn = in / rows;
+}
+
 // One order d of the split product over k-range [k0, k0 + kc):
 //   C (+)= 2^(ea[i] + eb[j] - 7(d+2)) sum_{p+q=d} A_p B_q^T
 // Persistent: warp 0 loads the slice tiles by TMA (rows p*mp + m0 of A's planes, q*np + n0 of
@@ -151,8 +164,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ntn = (n + BN - 1) / BN;
-  const int tiles = ((m + BM - 1) / BM) * ntn;
+  const int ntn = (n + BN - 1) / BN, ntm = (m + BM - 1) / BM;
+  const int tiles = ntm * ntn;
   const int ktiles = (kc + BK - 1) / BK;
   const int pairs = d + 1;  // (p, d - p) for p = 0..d
 
@@ -183,7 +196,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       int it = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+        int tmi, tni;
+        tile_coords(tile, ntm, ntn, tmi, tni);
+        const int m0 = tmi * BM, n0 = tni * BN;
         for (int pq = 0; pq < pairs && ok; ++pq)
           for (int kt = 0; kt < ktiles; ++kt, ++it) {
             const int s = it % STAGES;
@@ -239,7 +254,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int buf = lt & 1;
       if (!mbar_wait(&tfull[buf], (lt >> 1) & 1u, status)) break;
       tc::fence_after();
-      const int m0 = (tile / ntn) * BM, n0 = (tile % ntn) * BN;
+      int tmi, tni;
+      tile_coords(tile, ntm, ntn, tmi, tni);
+      const int m0 = tmi * BM, n0 = tni * BN;
       const int row0 = m0 + q * 32;
 #pragma unroll 1
       for (int cb = 0; cb < BN; cb += 32) {
