@@ -431,8 +431,12 @@ int rm_sgemm_tc(int passes, int transb, int64_t m, int64_t n, int64_t k, float a
   const bool fix_a = (reinterpret_cast<uintptr_t>(d_a) & 15) || (lda & 3);
   const bool fix_b = !transb || (reinterpret_cast<uintptr_t>(d_b) & 15) || (ldb & 3);
   const int64_t pa = round_up(k, 4), pb = round_up(k, 4);
+  // a rank-k update (three passes, k <= 256): the operands' low parts go to global memory once,
+  // and the kernel loads them beside the operands instead of forming them per output tile
+  const bool lo_g = passes == 3 && k <= 256;
   Arena ar;
   const size_t oa = fix_a ? ar.add((size_t)m * pa * 4) : 0, ob = fix_b ? ar.add((size_t)n * pb * 4) : 0;
+  const size_t oal = lo_g ? ar.add((size_t)m * pa * 4) : 0, obl = lo_g ? ar.add((size_t)n * pb * 4) : 0;
   Scratch sc;
   sc.stream = s;
   if (ar.total) RM_TRY(scratch_alloc(&sc.base, ar.total, s));
@@ -452,6 +456,13 @@ int rm_sgemm_tc(int passes, int transb, int64_t m, int64_t n, int64_t k, float a
     }
     b = sc.at<float>(ob);
     lb = pb;
+  }
+  if (lo_g) {
+    float* al = sc.at<float>(oal);
+    float* bl = sc.at<float>(obl);
+    RM_TRY(split_lo_f32(a, la, m, k, al, pa, s));
+    RM_TRY(split_lo_f32(b, lb, n, k, bl, pb, s));
+    return sgemm_tc_lo(m, n, k, alpha, a, la, al, pa, b, lb, bl, pb, beta, d_c, ldc, device_status(), s);
   }
   return sgemm_tc(passes, m, n, k, alpha, a, la, b, lb, beta, d_c, ldc, device_status(), s);
 }

@@ -482,8 +482,9 @@ struct LookAhead {
 };
 
 size_t getrf_lpp_f32_scratch_bytes(int64_t n) {
-  // linv, uinvt, a12t, u12t; each panel's row permutation (256 ints per panel)
-  return (2 * (size_t)kLppCols * kLppCols + 2 * (size_t)n * kLppCols) * sizeof(float) +
+  // linv, uinvt, a12t, u12t, the low parts of L21 and U12^T; each panel's row permutation
+  // (256 ints per panel)
+  return (2 * (size_t)kLppCols * kLppCols + 4 * (size_t)n * kLppCols) * sizeof(float) +
          (size_t)((n + kLppCols - 1) / kLppCols) * kLppRows * sizeof(int) + 2048;
 }
 
@@ -495,7 +496,9 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
   float* uinvt = linv + kLppCols * kLppCols;
   float* a12t = uinvt + kLppCols * kLppCols;   // rest x 128: A12^T
   float* u12t = a12t + (size_t)n * kLppCols;   // rest x 128: U12^T
-  int* plocal = reinterpret_cast<int*>(u12t + (size_t)n * kLppCols);
+  float* l21lo = u12t + (size_t)n * kLppCols;  // rest x 128: low parts of L21 (ld 128) ...
+  float* u12lo = l21lo + (size_t)n * kLppCols;  // ... and of U12^T, for the trailing update
+  int* plocal = reinterpret_cast<int*>(u12lo + (size_t)n * kLppCols);
   static bool set = false;
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(lpp_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLppSmem));
@@ -561,8 +564,11 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
     if (rest > nn) {
       RM_CUDA_TRY(cudaEventRecord(la.next_done, stream));
       RM_CUDA_TRY(cudaStreamWaitEvent(la.side, la.next_done, 0));
-      RM_TRY(sgemm_tc(3, rest, rest - nn, nb, -1.0f, l21, lda, u12t + (size_t)nn * kLppCols, kLppCols, 1.0f, a22 + nn,
-                      lda, status, la.side, nullptr, 0, device_sm_count() - kLookAheadSms));
+      // the panels' low parts once, then the update loads them beside the panels
+      RM_TRY(split_lo_f32(l21, lda, rest, nb, l21lo, kLppCols, la.side));
+      RM_TRY(split_lo_f32(u12t + (size_t)nn * kLppCols, kLppCols, rest - nn, nb, u12lo, kLppCols, la.side));
+      RM_TRY(sgemm_tc_lo(rest, rest - nn, nb, -1.0f, l21, lda, l21lo, kLppCols, u12t + (size_t)nn * kLppCols, kLppCols,
+                         u12lo, kLppCols, 1.0f, a22 + nn, lda, status, la.side, device_sm_count() - kLookAheadSms));
       RM_CUDA_TRY(cudaEventRecord(la.rest_done, la.side));
     }
   }

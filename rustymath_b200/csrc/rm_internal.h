@@ -39,6 +39,11 @@ struct SgemmOperands {
 };
 int sgemm_tc_pair(int passes, const SgemmOperands& x, const SgemmOperands& y, int64_t n, int64_t k, float alpha,
                   float beta, unsigned* status, cudaStream_t stream, int max_ctas = 0);
+// Three-pass C = alpha A B^T + beta C with the low parts of A and B (x - trunc_tf32(x), from
+// split_lo_f32) given in global memory, loaded beside A and B instead of formed per tile.
+int sgemm_tc_lo(int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* a_lo,
+                int64_t ldal, const float* b, int64_t ldb, const float* b_lo, int64_t ldbl, float beta, float* c,
+                int64_t ldc, unsigned* status, cudaStream_t stream, int max_ctas = 0);
 int transpose_f32(const float* src, int64_t lds, int64_t m, int64_t n, float* dst, int64_t ldd, cudaStream_t stream);
 int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStream_t stream);
 int split_lo_f32(const float* x, int64_t ldx, int64_t m, int64_t k, float* lo, int64_t ldl, cudaStream_t stream);

@@ -80,17 +80,21 @@ struct SgemmPart {
   int tiles;
 };
 
-template <int PASSES, bool TMA_EPI>
+// LO_G (three passes, one product): the low parts of A and B come from global memory
+// (tm_alo, tm_blo: same shapes and coordinates as A and B), loaded by TMA beside A and B, in
+// place of warps 6..9 forming them in shared memory.
+template <int PASSES, bool TMA_EPI, bool LO_G>
 __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
     sgemm_tc_kernel(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
                     const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_a2,
                     const __grid_constant__ CUtensorMap tm_b2, const __grid_constant__ CUtensorMap tm_c2,
+                    const __grid_constant__ CUtensorMap tm_alo, const __grid_constant__ CUtensorMap tm_blo,
                     const SgemmPart p1, const SgemmPart p2, int n, int k, float alpha, float beta,
                     unsigned* status) {
   using namespace tc;
   using C = Cfg<PASSES>;
   constexpr int S = C::STAGES;
-  constexpr int LOAD_BYTES = 2 * TILE_BYTES;
+  constexpr int LOAD_BYTES = (LO_G ? 4 : 2) * TILE_BYTES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   float* stg_all = reinterpret_cast<float*>(smem + S * C::STAGE_BYTES);
@@ -151,6 +155,10 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
         tma_prefetch_desc(&tm_a2);
         tma_prefetch_desc(&tm_b2);
       }
+      if (LO_G) {
+        tma_prefetch_desc(&tm_alo);
+        tma_prefetch_desc(&tm_blo);
+      }
       int it = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
@@ -170,6 +178,10 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
           mbar_arrive_expect_tx(&full[s], LOAD_BYTES);
           tma_load_2d(st, ma, &full[s], kt * BK, m0);
           tma_load_2d(st + TILE_BYTES, mb, &full[s], kt * BK, n0);
+          if (LO_G) {
+            tma_load_2d(st + 2 * TILE_BYTES, &tm_alo, &full[s], kt * BK, m0);
+            tma_load_2d(st + 3 * TILE_BYTES, &tm_blo, &full[s], kt * BK, n0);
+          }
         }
       }
       // the copies still in flight land before this thread leaves (bounded)
@@ -189,7 +201,7 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
         for (int kt = 0; kt < ktiles; ++kt, ++it) {
           const int s = it % S;
           const uint32_t par = (it / S) & 1u;
-          if (!mbar_wait(&full[s], par, status) || (PASSES == 3 && !mbar_wait(&lo_ready[s], par, status))) {
+          if (!mbar_wait(&full[s], par, status) || (PASSES == 3 && !LO_G && !mbar_wait(&lo_ready[s], par, status))) {
             ok = false;
             break;
           }
@@ -379,7 +391,7 @@ __global__ void __launch_bounds__(tc::Cfg<PASSES>::THREADS, 1)
         }
       }
     }
-  } else if (PASSES == 3) {
+  } else if (PASSES == 3 && !LO_G) {
     // ---------------- warps 6..9: the low parts of each stage
     const int t = threadIdx.x - 192;  // 0..127
     int it = 0;
@@ -448,21 +460,22 @@ int scale_f32(float* c, int64_t ldc, int64_t m, int64_t n, float beta, cudaStrea
   return RM_OK;
 }
 
-template <int PASSES, bool TMA_EPI>
+template <int PASSES, bool TMA_EPI, bool LO_G = false>
 static int launch_sgemm(const CUtensorMap* maps, const SgemmPart& p1, const SgemmPart& p2, int n, int k, float alpha,
                         float beta, unsigned* status, cudaStream_t stream, int max_ctas) {
   using C = tc::Cfg<PASSES>;
   static bool set = false;
   if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tc_kernel<PASSES, TMA_EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)C::SMEM));
+    RM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tc_kernel<PASSES, TMA_EPI, LO_G>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
     set = true;
   }
   const int64_t tiles = (int64_t)p1.tiles + p2.tiles;
   const int ctas = max_ctas > 0 ? std::min(max_ctas, device_sm_count()) : device_sm_count();
   const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctas);
-  RM_CUDA_TRY(launch_dependent(sgemm_tc_kernel<PASSES, TMA_EPI>, dim3(grid), dim3(C::THREADS), C::SMEM, stream, maps[0],
-                               maps[1], maps[2], maps[3], maps[4], maps[5], p1, p2, n, k, alpha, beta, status));
+  RM_CUDA_TRY(launch_dependent(sgemm_tc_kernel<PASSES, TMA_EPI, LO_G>, dim3(grid), dim3(C::THREADS), C::SMEM, stream,
+                               maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], maps[6], maps[7], p1, p2, n, k,
+                               alpha, beta, status));
   RM_LAUNCHED();
   return RM_OK;
 }
@@ -497,7 +510,7 @@ int sgemm_tc_pair(int passes, const SgemmOperands& x, const SgemmOperands& y, in
   if (y.m > 0) live[cnt++] = &y;
   if (cnt == 0) return RM_OK;
   const bool tma_epi = tma_epilogue_ok(*live[0], beta) && (cnt == 1 || tma_epilogue_ok(*live[1], beta));
-  CUtensorMap maps[6];
+  CUtensorMap maps[8];
   SgemmPart p[2];
   RM_TRY(prepare_part(*live[0], n, k, tma_epi, maps, &p[0]));
   if (cnt == 2) {
@@ -506,12 +519,32 @@ int sgemm_tc_pair(int passes, const SgemmOperands& x, const SgemmOperands& y, in
     memcpy(maps + 3, maps, 3 * sizeof(CUtensorMap));
     p[1] = {nullptr, 0, nullptr, 0, 0, 0};
   }
+  memcpy(maps + 6, maps, 2 * sizeof(CUtensorMap));  // no low parts from global memory
   const int ni = (int)n, ki = (int)k;
   if (passes == 3)
     return tma_epi ? launch_sgemm<3, true>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas)
                    : launch_sgemm<3, false>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas);
   return tma_epi ? launch_sgemm<1, true>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas)
                  : launch_sgemm<1, false>(maps, p[0], p[1], ni, ki, alpha, beta, status, stream, max_ctas);
+}
+
+int sgemm_tc_lo(int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* a_lo,
+                int64_t ldal, const float* b, int64_t ldb, const float* b_lo, int64_t ldbl, float beta, float* c,
+                int64_t ldc, unsigned* status, cudaStream_t stream, int max_ctas) {
+  if (m == 0 || n == 0) return RM_OK;
+  if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || k == 0) return RM_BAD_ARG;
+  const SgemmOperands x{m, a, lda, b, ldb, c, ldc, nullptr, 0};
+  const bool tma_epi = tma_epilogue_ok(x, beta);
+  CUtensorMap maps[8];
+  SgemmPart p[2];
+  RM_TRY(prepare_part(x, n, k, tma_epi, maps, &p[0]));
+  memcpy(maps + 3, maps, 3 * sizeof(CUtensorMap));
+  p[1] = {nullptr, 0, nullptr, 0, 0, 0};
+  RM_TRY(make_tensor_map_2d(&maps[6], a_lo, 4, k, m, ldal * 4, tc::BK, tc::BM, true));
+  RM_TRY(make_tensor_map_2d(&maps[7], b_lo, 4, k, n, ldbl * 4, tc::BK, tc::BN, true));
+  return tma_epi ? launch_sgemm<3, true, true>(maps, p[0], p[1], (int)n, (int)k, alpha, beta, status, stream, max_ctas)
+                 : launch_sgemm<3, false, true>(maps, p[0], p[1], (int)n, (int)k, alpha, beta, status, stream,
+                                                max_ctas);
 }
 
 int sgemm_tc(int passes, int64_t m, int64_t n, int64_t k, float alpha, const float* a, int64_t lda, const float* b,
