@@ -691,9 +691,11 @@ def main():
                     "achieved": gbs, "peak": peak_hbm(), "unit": "GB/s", "frac": gbs / peak_hbm(),
                     "peak_source": peak_hbm_source()[1],
                     "bytes_per_launch": bytes_upd, "launch_us": 1e6 * t_upd, "tf32_tflops": tf32_tflops,
-                    "traffic": 268.47e6 + 201.07e6,
+                    "traffic": 276.83e6 + 200.59e6,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch at full size "
-                                      "(bench.py --workload update, the 4th launch)"}
+                                      "(bench.py --workload update, the 4th GEMM launch)",
+                    "timing_note": "launch_us is the rm_sgemm_tc call: the two low-part splits of the panels "
+                                   "(2 x 4 MB) and the GEMM launch"}
         peak64 = gemm_peak_f64(torch, dev)
         achieved, t_launch = time_dgemm_update(torch, lib, dev, n)
         roofline["plain_path_dgemm"] = {"bound": "tensor", "kernel": "dgemm_kernel<128x128> rank-128 update",
