@@ -135,7 +135,7 @@ __global__ void split_cols_kernel(const double* __restrict__ b, int64_t ldb, int
 // down a band's rows first, then across its columns, so that the ~148 tiles in flight at once
 // read about kBand row panels of A's slices and 148 / kBand column panels of B's (some tens of
 // MB, resident in L2) instead of one row panel and 148 column panels.
-constexpr int kBand = 16;
+constexpr int kBand = 8;
 __device__ __forceinline__ void tile_coords(int t, int ntm, int ntn, int& tm, int& tn) {
   const int per_band = kBand * ntn;
   const int band = t / per_band, in = t - band * per_band;
