@@ -15,7 +15,9 @@
 //       dgemm            : the block's later columns below the leaf -= L21 U12
 //     swap_trsm_kernel   : the block's swaps on every column outside it, and perm
 //     invert_unit_lower  : L11^-1 of the block's diagonal
-//     dgemm              : U12 = L11^-1 A12 (in place), then A22 -= L21 U12
+//     dgemm              : U12 = L11^-1 A12 (in place), then A22 -= L21 U12: the next
+//                          block's 128 columns first; for n >= 1024 the rest runs on a side
+//                          stream while the next block's leaves factor (look-ahead)
 //
 // The pivot rule is the reference's `largest` (factor.rs:476): the first row of greatest
 // magnitude, NaN never chosen, the diagonal itself when every candidate is NaN; a zero
@@ -502,14 +504,54 @@ __global__ void iota_kernel(int64_t* perm, int64_t n) {
 
 size_t getrf_f64_scratch_bytes(int64_t n) { return (size_t)kOuter * kOuter * sizeof(double) + 256; }
 
+namespace {
+// The look-ahead's streams: the critical chain (hp) at the device's highest stream priority, the
+// rest of each trailing update (side) at its lowest, so that the chain's panel clusters take
+// SMs first as the update's tiles finish. Released on return (queued work completes first).
+struct F64LookAhead {
+  cudaStream_t hp = nullptr, side = nullptr;
+  cudaEvent_t next_done = nullptr, rest_done = nullptr, entry = nullptr;
+  int open() {
+    int least = 0, greatest = 0;
+    RM_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    RM_CUDA_TRY(cudaStreamCreateWithPriority(&hp, cudaStreamNonBlocking, greatest));
+    RM_CUDA_TRY(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, least));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&next_done, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&rest_done, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&entry, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventRecord(rest_done, side));  // complete at first, so the first wait passes
+    return RM_OK;
+  }
+  ~F64LookAhead() {
+    if (next_done) cudaEventDestroy(next_done);
+    if (rest_done) cudaEventDestroy(rest_done);
+    if (entry) cudaEventDestroy(entry);
+    if (hp) cudaStreamDestroy(hp);
+    if (side) cudaStreamDestroy(side);
+  }
+};
+}  // namespace
+
 int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm, void* scratch, unsigned* status,
-              cudaStream_t stream) {
+              cudaStream_t caller) {
   if (n64 <= 0) return RM_OK;
   if (n64 > INT32_MAX / 2) return RM_BAD_ARG;
   const int n = (int)n64;
   double* linv = reinterpret_cast<double*>(scratch);
-  iota_kernel<<<std::max(1, std::min(n / 256 + 1, 1024)), 256, 0, stream>>>(perm, n);
+  iota_kernel<<<std::max(1, std::min(n / 256 + 1, 1024)), 256, 0, caller>>>(perm, n);
   RM_LAUNCHED();
+  // Look-ahead (n >= 1024): each trailing update does the next block's 128 columns first, on
+  // the chain's stream; the rest runs on a side stream while the next block's leaves factor.
+  // Only the block's row swaps on the columns right of it wait for that rest (it writes them).
+  F64LookAhead la;
+  const bool ahead = n >= 1024;
+  cudaStream_t stream = caller;
+  if (ahead) {
+    RM_TRY(la.open());
+    RM_CUDA_TRY(cudaEventRecord(la.entry, caller));
+    RM_CUDA_TRY(cudaStreamWaitEvent(la.hp, la.entry, 0));
+    stream = la.hp;
+  }
   for (int J0 = 0; J0 < n; J0 += kOuter) {
     const int nb = std::min(kOuter, n - J0);
     const int J1 = J0 + nb;
@@ -525,7 +567,9 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
                             status, stream));
       }
     }
-    // the block's swaps on every other column, and the row permutation
+    // the block's swaps on every other column, and the row permutation (after the rest of the
+    // last trailing update, which writes the columns right of this block)
+    if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
     RM_TRY(launch_swap<double>(w, ldw, J0, nb, ipiv, 0, J0, J1, n, 0, 0, perm, stream));
     if (J1 < n) {
       invert_unit_lower_kernel<double><<<1, 256, 0, stream>>>(w, ldw, J0, nb, linv);
@@ -533,9 +577,28 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
       double* a12 = w + (int64_t)J0 * ldw + J1;
       RM_TRY(dgemm_device(false, false, nb, n - J1, nb, 1.0, linv, kOuter, a12, ldw, 0.0, a12, ldw, status, stream,
                           /*force_wide_m=*/true));
-      RM_TRY(dgemm_device(false, false, n - J1, n - J1, nb, -1.0, w + (int64_t)J1 * ldw + J0, ldw, a12, ldw, 1.0,
-                          w + (int64_t)J1 * ldw + J1, ldw, status, stream));
+      const double* l21 = w + (int64_t)J1 * ldw + J0;
+      double* a22 = w + (int64_t)J1 * ldw + J1;
+      const int rest = n - J1;
+      if (!ahead) {
+        RM_TRY(dgemm_device(false, false, rest, rest, nb, -1.0, l21, ldw, a12, ldw, 1.0, a22, ldw, status, stream));
+        continue;
+      }
+      const int nn = std::min(kOuter, rest);
+      RM_TRY(dgemm_device(false, false, rest, nn, nb, -1.0, l21, ldw, a12, ldw, 1.0, a22, ldw, status, stream));
+      if (rest > nn) {
+        RM_CUDA_TRY(cudaEventRecord(la.next_done, stream));
+        RM_CUDA_TRY(cudaStreamWaitEvent(la.side, la.next_done, 0));
+        RM_TRY(dgemm_device(false, false, rest, rest - nn, nb, -1.0, l21, ldw, a12 + nn, ldw, 1.0, a22 + nn, ldw, status,
+                            la.side));
+        RM_CUDA_TRY(cudaEventRecord(la.rest_done, la.side));
+      }
     }
+  }
+  if (ahead) {
+    RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
+    RM_CUDA_TRY(cudaEventRecord(la.entry, stream));  // the caller's stream continues after both
+    RM_CUDA_TRY(cudaStreamWaitEvent(caller, la.entry, 0));
   }
   return RM_OK;
 }
