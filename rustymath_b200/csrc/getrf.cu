@@ -14,7 +14,7 @@
 //                          U = L^-1 A for the leaf's rows of the block's later columns
 //       dgemm            : the block's later columns below the leaf -= L21 U12
 //     swap_trsm_kernel   : the block's swaps on every column outside it, and perm
-//     invert_unit_lower  : L11^-1 of the block's diagonal
+//     invert_unit_lower_f64 : L11^-1 of the block's diagonal (4 CTAs, a 32-column block each)
 //     dgemm              : U12 = L11^-1 A12 (in place), then A22 -= L21 U12: the next
 //                          block's 128 columns first; for n >= 1024 the rest runs on a side
 //                          stream while the next block's leaves factor (look-ahead)
@@ -361,60 +361,6 @@ __global__ void __launch_bounds__(kSwapThreads)
   }
 }
 
-// ------------------------------------------------------------------ L11^-1 of an outer block
-// out (ld kOuter) = inverse of the unit lower triangle of W[j0..j0+nb, j0..j0+nb), nb <= kOuter.
-// Diagonal 32x32 blocks invert by column substitution (a warp each, a lane per column);
-// block (b, a) below them is -D_b^-1 * sum_{c=a..b-1} L_bc X_ca, in order of b - a. L is
-// read from W (it stays in L1/L2); X is built in `out`.
-template <typename T>
-__global__ void __launch_bounds__(256) invert_unit_lower_kernel(const T* __restrict__ w, int64_t ldw, int j0, int nb,
-                                                                T* __restrict__ out) {
-  __shared__ T tmp[kLeaf][kLeaf + 1];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const T* l = w + (int64_t)j0 * ldw + j0;
-  auto L = [&](int r, int c) -> T { return (r < nb && c < nb && c < r) ? l[(int64_t)r * ldw + c] : T(0); };
-  for (int e = tid; e < kOuter * kOuter; e += 256) out[e] = T(0);
-  __syncthreads();
-  const int nblk = (nb + kLeaf - 1) / kLeaf;
-  if (warp < nblk) {
-    const int b0 = warp * kLeaf;
-    // column `lane` of D^-1: x_i = -sum_{k<i} D_ik x_k for i > lane, x_lane = 1
-    T x[kLeaf];
-#pragma unroll
-    for (int i = 0; i < kLeaf; ++i) {
-      T s = i == lane ? T(1) : T(0);
-#pragma unroll
-      for (int k = 0; k < i; ++k) s = fma(-L(b0 + i, b0 + k), x[k], s);
-      x[i] = i < lane ? T(0) : s;
-    }
-#pragma unroll
-    for (int i = 0; i < kLeaf; ++i)
-      if (b0 + i < nb && b0 + lane < nb) out[(b0 + i) * kOuter + b0 + lane] = x[i];
-  }
-  __syncthreads();
-  for (int gap = 1; gap < nblk; ++gap) {
-    for (int a = 0; a + gap < nblk; ++a) {
-      const int b = a + gap, rb = b * kLeaf, ca = a * kLeaf;
-      // tmp = sum_{c=a..b-1} L_bc X_ca  (32x32)
-      for (int e = tid; e < kLeaf * kLeaf; e += 256) {
-        const int i = e / kLeaf, j = e % kLeaf;
-        T s = T(0);
-        for (int k = ca; k < rb; ++k) s = fma(L(rb + i, k), out[k * kOuter + ca + j], s);
-        tmp[i][j] = s;
-      }
-      __syncthreads();
-      // X_ba = -D_b^-1 tmp, with D_b^-1 (unit lower) in out's diagonal block b
-      for (int e = tid; e < kLeaf * kLeaf; e += 256) {
-        const int i = e / kLeaf, j = e % kLeaf;
-        T s = T(0);
-        for (int k = 0; k <= i; ++k) s = fma(out[(rb + i) * kOuter + rb + k], tmp[k][j], s);
-        if (rb + i < nb && ca + j < nb) out[(rb + i) * kOuter + ca + j] = -s;
-      }
-      __syncthreads();
-    }
-  }
-}
-
 // ------------------------------------------------------------------ driver
 
 // The largest cluster (<= kMaxCluster CTAs of kPanelSmemBudget bytes) this device can place.
@@ -497,6 +443,68 @@ static int launch_swap(T* w, int64_t ldw, int j0, int jb, const int64_t* ipiv, i
   return RM_OK;
 }
 
+// L11^-1 of the unit lower triangle of the nb x nb diagonal block at (j0, j0) (row-major,
+// ld kOuter, zeros above the diagonal; identity beyond nb), a 32-column block of it per CTA
+// (4 CTAs), everything in shared memory: CTA a forms X_aa = D_a^-1 and then, block row by block
+// row, X_ba = -D_b^-1 sum_{c=a..b-1} L_bc X_ca; the diagonal blocks' inverses D_b^-1 first, a
+// warp each, a lane per column (forward substitution).
+constexpr int kInvS = kOuter + 1;
+constexpr size_t kInv64Smem = ((size_t)kOuter * kInvS + (size_t)(4 * kLeaf + kOuter + kLeaf) * (kLeaf + 1)) *
+                              sizeof(double);
+
+__global__ void __launch_bounds__(256) invert_unit_lower_f64_kernel(const double* __restrict__ w, int64_t ldw, int j0,
+                                                                    int nb, double* __restrict__ out) {
+  extern __shared__ __align__(16) uint8_t smraw[];
+  double(*M)[kInvS] = reinterpret_cast<double(*)[kInvS]>(smraw);
+  double(*Y)[kLeaf + 1] = reinterpret_cast<double(*)[kLeaf + 1]>(smraw + (size_t)kOuter * kInvS * sizeof(double));
+  double(*X)[kLeaf + 1] = Y + 4 * kLeaf;  // the column block, rows 0..127
+  double(*Tq)[kLeaf + 1] = X + kOuter;     // 32 x 33
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ab = blockIdx.x, a0 = kLeaf * ab;
+  const double* l = w + (int64_t)j0 * ldw + j0;
+  // L from row and column a0 on (strictly lower part; unit diagonal implied)
+  for (int i = a0 + warp; i < kOuter; i += 8)
+    for (int k = a0 + lane; k < kOuter; k += 32) M[i][k] = (i < nb && k < nb && k < i) ? l[(int64_t)i * ldw + k] : 0.0;
+  __syncthreads();
+  if (warp < 4 - ab) {  // Y_b = D_b^-1, b = ab + warp
+    const int b0 = a0 + kLeaf * warp;
+    double x[kLeaf];
+#pragma unroll
+    for (int i = 0; i < kLeaf; ++i) {
+      double acc = i == lane ? 1.0 : 0.0;
+#pragma unroll
+      for (int k2 = 0; k2 < i; ++k2) acc = fma(-M[b0 + i][b0 + k2], x[k2], acc);
+      x[i] = i < lane ? 0.0 : acc;
+    }
+#pragma unroll
+    for (int i = 0; i < kLeaf; ++i) Y[b0 + i][lane] = x[i];
+  }
+  __syncthreads();
+  for (int e = tid; e < kLeaf * kLeaf; e += 256) X[a0 + (e >> 5)][e & 31] = Y[a0 + (e >> 5)][e & 31];
+  __syncthreads();
+  const int ti = tid >> 4, tj = tid & 15;  // rows ti, ti + 16 and columns tj, tj + 16 of a 32 x 32 block
+  for (int b = ab + 1; b < 4; ++b) {
+    const int r0 = kLeaf * b + ti, r1 = r0 + 16;
+    double t00 = 0.0, t01 = 0.0, t10 = 0.0, t11 = 0.0;
+#pragma unroll 4
+    for (int k = a0; k < kLeaf * b; ++k) {
+      const double m0 = M[r0][k], m1 = M[r1][k], x0 = X[k][tj], x1 = X[k][tj + 16];
+      t00 = fma(m0, x0, t00), t01 = fma(m0, x1, t01), t10 = fma(m1, x0, t10), t11 = fma(m1, x1, t11);
+    }
+    Tq[ti][tj] = t00, Tq[ti][tj + 16] = t01, Tq[ti + 16][tj] = t10, Tq[ti + 16][tj + 16] = t11;
+    __syncthreads();
+    t00 = t01 = t10 = t11 = 0.0;
+#pragma unroll 4
+    for (int k2 = 0; k2 < kLeaf; ++k2) {
+      const double y0 = Y[r0][k2], y1 = Y[r1][k2], u0 = Tq[k2][tj], u1 = Tq[k2][tj + 16];
+      t00 = fma(y0, u0, t00), t01 = fma(y0, u1, t01), t10 = fma(y1, u0, t10), t11 = fma(y1, u1, t11);
+    }
+    X[r0][tj] = -t00, X[r0][tj + 16] = -t01, X[r1][tj] = -t10, X[r1][tj + 16] = -t11;
+    __syncthreads();
+  }
+  for (int rr = warp; rr < kOuter; rr += 8) out[rr * kOuter + a0 + lane] = rr >= a0 ? X[rr][lane] : 0.0;
+}
+
 __global__ void iota_kernel(int64_t* perm, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     perm[i] = i;
@@ -543,6 +551,12 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
   // Look-ahead (n >= 1024): each trailing update does the next block's 128 columns first, on
   // the chain's stream; the rest runs on a side stream while the next block's leaves factor.
   // Only the block's row swaps on the columns right of it wait for that rest (it writes them).
+  static bool inv_set = false;
+  if (!inv_set) {
+    RM_CUDA_TRY(cudaFuncSetAttribute(invert_unit_lower_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kInv64Smem));
+    inv_set = true;
+  }
   F64LookAhead la;
   const bool ahead = n >= 1024;
   cudaStream_t stream = caller;
@@ -572,7 +586,7 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
     if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
     RM_TRY(launch_swap<double>(w, ldw, J0, nb, ipiv, 0, J0, J1, n, 0, 0, perm, stream));
     if (J1 < n) {
-      invert_unit_lower_kernel<double><<<1, 256, 0, stream>>>(w, ldw, J0, nb, linv);
+      invert_unit_lower_f64_kernel<<<kOuter / kLeaf, 256, kInv64Smem, stream>>>(w, ldw, J0, nb, linv);
       RM_LAUNCHED();
       double* a12 = w + (int64_t)J0 * ldw + J1;
       RM_TRY(dgemm_device(false, false, nb, n - J1, nb, 1.0, linv, kOuter, a12, ldw, 0.0, a12, ldw, status, stream,
