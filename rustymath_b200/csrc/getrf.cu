@@ -265,14 +265,18 @@ __global__ void __launch_bounds__(kSwapThreads)
   __shared__ int count;
   __shared__ T buf[2 * kMaxSwaps][kSwapCols + 1];
   __shared__ T lblk[kLeaf][kLeaf + 1];
+  __shared__ int ipv[kMaxSwaps];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the swaps' targets, all at once (the loop below is sequential over them)
+  for (int q = tid; q < jb; q += kSwapThreads) ipv[q] = (int)ipiv[j0 + q];
+  __syncthreads();
 
   // ---- the net effect of the swaps: row pos[e] receives the old row src[e]
   if (warp == 0) {
     for (int q = lane; q < jb; q += 32) pos[q] = src[q] = j0 + q;
     int cntE = jb;
     for (int i = 0; i < jb; ++i) {
-      const int d = j0 + i, p = (int)ipiv[d];
+      const int d = j0 + i, p = ipv[i];
       if (p == d) continue;
       int e;
       if (p < j0 + jb) {
