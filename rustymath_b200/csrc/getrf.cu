@@ -231,6 +231,7 @@ __global__ void __launch_bounds__(kPanelThreads)
           T l = at(lr, c);
           l = sub ? l / pivot : l * r;
           at(lr, c) = l;
+#pragma unroll 8
           for (int cc = c + 1; cc < jb; ++cc) at(lr, cc) = fma(l, -sh->piv[cc], at(lr, cc));
         }
       }
