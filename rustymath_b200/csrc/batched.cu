@@ -215,6 +215,7 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
       // the rows not chosen yet: later columns -= L(row, panel) U12
       if (active) {
         T* rrow = W + (int64_t)r * ld + rc0;
+#pragma unroll 4
         for (int j = 0; j < rcols; ++j) {
           T acc = rrow[j];
 #pragma unroll
