@@ -335,9 +335,11 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
   }
   for (int r = warp; r < n; r += WARPS) {
     const double* ar = a + (int64_t)r * n;
+    const double bv = lane < k ? b[(int64_t)r * k + lane] : 0.0;  // in flight beside the row
     double acc[KMAX], asum = 0.0;
 #pragma unroll
     for (int c = 0; c < KMAX; ++c) acc[c] = 0.0;
+#pragma unroll 4
     for (int j = lane; j < n; j += 32) {
       const double av = __ldg(ar + j);
       asum += fabs(av);
@@ -358,7 +360,6 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
 #pragma unroll
       for (int c = 0; c < KMAX; ++c)
         if (c == lane) mine = acc[c];
-      const double bv = b[(int64_t)r * k + lane];
       const double rv = bv - mine;
       sm.rs[r][lane] = rv;
 #pragma unroll
