@@ -656,6 +656,7 @@ __device__ double bresidual_t(const double* __restrict__ a, const double* __rest
     double acc[KMAX];
 #pragma unroll
     for (int c = 0; c < KMAX; ++c) acc[c] = 0.0;
+#pragma unroll 4
     for (int i = 0; i < n; ++i) {
       const double av = __ldg(a + (int64_t)i * n + t);  // column t: coalesced across threads
       asum += fabs(av);
