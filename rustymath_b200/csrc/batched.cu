@@ -230,8 +230,8 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
 
 // Solves L U x = P v: thread r holds v (its row's k right-hand sides) on entry and x[my_pos]
 // on return. W holds the implicitly pivoted factors of bfactor<T, NB>.
-template <typename T, int NB>
-__device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T (&v)[KMAX]) {
+template <typename T, int NB, int KK>
+__device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T (&v)[KK]) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r = tid;
   const T* row = W + (int64_t)r * ld;
@@ -240,7 +240,7 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
     const int nbj = min(NB, n - J);
     if (my_pos >= J && my_pos < J + nbj)
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
+      for (int c = 0; c < KK; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
     __syncthreads();
     if (warp < k) {  // a warp per right-hand side: column c = warp, lane = row of the block
       const int c = warp;
@@ -266,12 +266,12 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
           if (q < nbj) {
             const T l = row[J + q];
 #pragma unroll
-            for (int c = 0; c < KMAX; ++c)
+            for (int c = 0; c < KK; ++c)
               if (c < k) v[c] = fma(-l, (T)sm.vsm[q][c], v[c]);
           }
       } else if (my_pos >= J) {
 #pragma unroll
-        for (int c = 0; c < KMAX; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
+        for (int c = 0; c < KK; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
       }
     }
     __syncthreads();
@@ -282,7 +282,7 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
     const int nbj = min(NB, n - J);
     if (my_pos >= J && my_pos < J + nbj)
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
+      for (int c = 0; c < KK; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
     __syncthreads();
     if (warp < k) {  // a warp per right-hand side
       const int c = warp;
@@ -309,12 +309,12 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
           if (q < nbj) {
             const T u = row[J + q];
 #pragma unroll
-            for (int c = 0; c < KMAX; ++c)
+            for (int c = 0; c < KK; ++c)
               if (c < k) v[c] = fma(-u, (T)sm.vsm[q][c], v[c]);
           }
       } else if (my_pos >= J && my_pos < J + nbj) {
 #pragma unroll
-        for (int c = 0; c < KMAX; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
+        for (int c = 0; c < KK; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
       }
     }
     __syncthreads();
@@ -324,46 +324,47 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
 // sm.rs = b - A sm.xs for the n x n row-major a (a warp per row, lanes along it) and returns
 // the normwise backward error (NaN if a residual is NaN). The first call (sm.anorm < 0)
 // also forms ||A||_inf and ||b_c||_inf.
+template <int KK>
 __device__ double bresidual(const double* __restrict__ a, const double* __restrict__ b, int n, int k, Smem& sm) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool first = sm.anorm < 0.0;
-  double rmax[KMAX], bmax[KMAX], xmax[KMAX], amax = 0.0;
+  double rmax[KK], bmax[KK], xmax[KK], amax = 0.0;
 #pragma unroll
-  for (int c = 0; c < KMAX; ++c) {
+  for (int c = 0; c < KK; ++c) {
     rmax[c] = bmax[c] = 0.0;
     xmax[c] = tid < n ? fabs(sm.xs[tid][c]) : 0.0;
   }
   for (int r = warp; r < n; r += WARPS) {
     const double* ar = a + (int64_t)r * n;
     const double bv = lane < k ? b[(int64_t)r * k + lane] : 0.0;  // in flight beside the row
-    double acc[KMAX], asum = 0.0;
+    double acc[KK], asum = 0.0;
 #pragma unroll
-    for (int c = 0; c < KMAX; ++c) acc[c] = 0.0;
+    for (int c = 0; c < KK; ++c) acc[c] = 0.0;
 #pragma unroll 4
     for (int j = lane; j < n; j += 32) {
       const double av = __ldg(ar + j);
       asum += fabs(av);
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c)
+      for (int c = 0; c < KK; ++c)
         if (c < k) acc[c] = fma(av, sm.xs[j][c], acc[c]);
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
       asum += __shfl_xor_sync(0xffffffffu, asum, off);
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c)
+      for (int c = 0; c < KK; ++c)
         if (c < k) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
     }
     amax = fmax(amax, asum);
     if (lane < k) {
       double mine = 0.0;
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c)
+      for (int c = 0; c < KK; ++c)
         if (c == lane) mine = acc[c];
       const double rv = bv - mine;
       sm.rs[r][lane] = rv;
 #pragma unroll
-      for (int c = 0; c < KMAX; ++c)
+      for (int c = 0; c < KK; ++c)
         if (c == lane) {
           rmax[c] = (fabs(rv) > rmax[c] || rv != rv) ? fabs(rv) : rmax[c];
           bmax[c] = fmax(bmax[c], fabs(bv));
@@ -372,7 +373,7 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
   }
   // the lanes of a warp hold different columns: combine per warp, then across warps
 #pragma unroll
-  for (int c = 0; c < KMAX; ++c) {
+  for (int c = 0; c < KK; ++c) {
     double rv = rmax[c], bv = bmax[c], xv = xmax[c];
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
@@ -385,7 +386,7 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
   }
   if (lane == 0) {
 #pragma unroll
-    for (int c = 0; c < KMAX; ++c) {
+    for (int c = 0; c < KK; ++c) {
       sm.red[warp][c] = rmax[c];
       sm.red[warp][KMAX + c] = bmax[c];
       sm.red[warp][2 * KMAX + c] = xmax[c];
@@ -448,34 +449,84 @@ struct Batch {
   int* ftype;          // per system: 0 when W holds float32 factors, 1 for float64
 };
 
-template <typename T, int NB>
+template <typename T, int NB, int KK>
 __device__ bool factor_and_solve(Batch& bt, Smem& sm, int n, int k, int ld, T* W, const double* a, const double* b,
                                  int& my_pos) {
   load_w<T>(a, n, W, ld);
   if (threadIdx.x == 0) sm.zero_pivot = 0;
   __syncthreads();
   bfactor<T, NB>(W, ld, n, sm, my_pos);
-  T v[KMAX];
+  T v[KK];
 #pragma unroll
-  for (int c = 0; c < KMAX; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)b[(int64_t)threadIdx.x * k + c] : T(0);
-  bsolve<T, NB>(W, ld, n, k, sm, my_pos, v);
+  for (int c = 0; c < KK; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)b[(int64_t)threadIdx.x * k + c] : T(0);
+  bsolve<T, NB, KK>(W, ld, n, k, sm, my_pos, v);
   if (my_pos >= 0)
 #pragma unroll
-    for (int c = 0; c < KMAX; ++c) sm.xs[my_pos][c] = (double)v[c];
+    for (int c = 0; c < KK; ++c) sm.xs[my_pos][c] = (double)v[c];
   __syncthreads();
   return sm.zero_pivot == 0;
 }
 
-template <typename T, int NB>
+template <typename T, int NB, int KK>
 __device__ void correct(Batch& bt, Smem& sm, int n, int k, int ld, const T* W, int my_pos) {
-  T v[KMAX];
+  T v[KK];
 #pragma unroll
-  for (int c = 0; c < KMAX; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)sm.rs[threadIdx.x][c] : T(0);
-  bsolve<T, NB>(W, ld, n, k, sm, my_pos, v);
+  for (int c = 0; c < KK; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)sm.rs[threadIdx.x][c] : T(0);
+  bsolve<T, NB, KK>(W, ld, n, k, sm, my_pos, v);
   if (my_pos >= 0)
 #pragma unroll
-    for (int c = 0; c < KMAX; ++c) sm.xs[my_pos][c] += (double)v[c];
+    for (int c = 0; c < KK; ++c) sm.xs[my_pos][c] += (double)v[c];
   __syncthreads();
+}
+
+// One system with at most KK right-hand sides (the solves and residuals loop over KK columns).
+template <int KK>
+__device__ void solve_system(Batch& bt, Smem& sm, int n, int k, int nb, int ld, const double* a, const double* b,
+                             unsigned char* w, int& my_pos, int& iters, int& flags, double& berr, bool& done) {
+  if (bt.method == RM_METHOD_F32_IR) {
+    float* W = reinterpret_cast<float*>(w);
+    if (nb == 32) factor_and_solve<float, 32, KK>(bt, sm, n, k, ld, W, a, b, my_pos);
+    else factor_and_solve<float, 16, KK>(bt, sm, n, k, ld, W, a, b, my_pos);
+    const double tol = bt.tol > 0.0 ? bt.tol : (double)n * 0x1.0p-53;
+    double prev = INFINITY;
+    for (;;) {
+      berr = bresidual<KK>(a, b, n, k, sm);
+      if (berr <= tol) {
+        done = true;
+        break;
+      }
+      if (!(berr < 0.5 * prev) || iters == bt.max_it) break;
+      prev = berr;
+      if (nb == 32) correct<float, 32, KK>(bt, sm, n, k, ld, W, my_pos);
+      else correct<float, 16, KK>(bt, sm, n, k, ld, W, my_pos);
+      ++iters;
+    }
+    if (!done) flags |= bt.fallback ? FLAG_FELL_BACK : FLAG_NO_CONVERGENCE;
+  }
+  if (!done && (bt.method != RM_METHOD_F32_IR || bt.fallback)) {
+    double* W = reinterpret_cast<double*>(w);
+    const bool nonzero = factor_and_solve<double, 16, KK>(bt, sm, n, k, ld, W, a, b, my_pos);
+    berr = bresidual<KK>(a, b, n, k, sm);
+    // rustymath's `regular`: every |u_ii| > eps * n * max|a| (a NaN pivot counts as regular)
+    __shared__ int irregular;
+    if (threadIdx.x == 0) irregular = nonzero ? 0 : 1;
+    __syncthreads();
+    double amax = 0.0;
+    for (int e = threadIdx.x; e < n * n; e += THREADS) amax = fmax(amax, fabs(a[e]));
+#pragma unroll
+    for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+    if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5][0] = amax;
+    __syncthreads();
+    double big = 0.0;
+    for (int q = 0; q < WARPS; ++q) big = fmax(big, sm.red[q][0]);
+    if (my_pos >= 0) {
+      const double u = W[(int64_t)threadIdx.x * ld + my_pos];
+      if (fabs(u) <= DBL_EPSILON * n * big) atomicOr(&irregular, 1);
+    }
+    __syncthreads();
+    if (irregular) flags |= FLAG_NOT_REGULAR;
+    __syncthreads();
+  }
 }
 
 __global__ void __launch_bounds__(THREADS, 2) batch_solve_kernel(Batch bt) {
@@ -499,50 +550,9 @@ __global__ void __launch_bounds__(THREADS, 2) batch_solve_kernel(Batch bt) {
     int my_pos = -1, iters = 0, flags = 0;
     double berr = 0.0;
     bool done = false;
-    if (bt.method == RM_METHOD_F32_IR) {
-      float* W = reinterpret_cast<float*>(w);
-      if (nb == 32) factor_and_solve<float, 32>(bt, sm, n, k, ld, W, a, b, my_pos);
-      else factor_and_solve<float, 16>(bt, sm, n, k, ld, W, a, b, my_pos);
-      const double tol = bt.tol > 0.0 ? bt.tol : (double)n * 0x1.0p-53;
-      double prev = INFINITY;
-      for (;;) {
-        berr = bresidual(a, b, n, k, sm);
-        if (berr <= tol) {
-          done = true;
-          break;
-        }
-        if (!(berr < 0.5 * prev) || iters == bt.max_it) break;
-        prev = berr;
-        if (nb == 32) correct<float, 32>(bt, sm, n, k, ld, W, my_pos);
-        else correct<float, 16>(bt, sm, n, k, ld, W, my_pos);
-        ++iters;
-      }
-      if (!done) flags |= bt.fallback ? FLAG_FELL_BACK : FLAG_NO_CONVERGENCE;
-    }
-    if (!done && (bt.method != RM_METHOD_F32_IR || bt.fallback)) {
-      double* W = reinterpret_cast<double*>(w);
-      const bool nonzero = factor_and_solve<double, 16>(bt, sm, n, k, ld, W, a, b, my_pos);
-      berr = bresidual(a, b, n, k, sm);
-      // rustymath's `regular`: every |u_ii| > eps * n * max|a| (a NaN pivot counts as regular)
-      __shared__ int irregular;
-      if (threadIdx.x == 0) irregular = nonzero ? 0 : 1;
-      __syncthreads();
-      double amax = 0.0;
-      for (int e = threadIdx.x; e < n * n; e += THREADS) amax = fmax(amax, fabs(a[e]));
-#pragma unroll
-      for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
-      if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5][0] = amax;
-      __syncthreads();
-      double big = 0.0;
-      for (int q = 0; q < WARPS; ++q) big = fmax(big, sm.red[q][0]);
-      if (my_pos >= 0) {
-        const double u = W[(int64_t)threadIdx.x * ld + my_pos];
-        if (fabs(u) <= DBL_EPSILON * n * big) atomicOr(&irregular, 1);
-      }
-      __syncthreads();
-      if (irregular) flags |= FLAG_NOT_REGULAR;
-      __syncthreads();
-    }
+    if (k <= 2) solve_system<2>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    else if (k <= 4) solve_system<4>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    else solve_system<KMAX>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
     // x (row-major n x k) from xs, by unknown; the factors' row order and type stay for the adjoint
     for (int e = threadIdx.x; e < n * k; e += THREADS) x[e] = sm.xs[e / k][e % k];
     for (int i = threadIdx.x; i < n; i += THREADS) bt.piv[bt.p_off[s] + i] = sm.piv[i];
