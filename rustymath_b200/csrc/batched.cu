@@ -550,7 +550,8 @@ __global__ void __launch_bounds__(THREADS, 2) batch_solve_kernel(Batch bt) {
     int my_pos = -1, iters = 0, flags = 0;
     double berr = 0.0;
     bool done = false;
-    if (k <= 2) solve_system<2>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    if (k <= 1) solve_system<1>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    else if (k <= 2) solve_system<2>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
     else if (k <= 4) solve_system<4>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
     else solve_system<KMAX>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
     // x (row-major n x k) from xs, by unknown; the factors' row order and type stay for the adjoint
