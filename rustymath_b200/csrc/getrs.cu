@@ -399,22 +399,31 @@ static int launch_trsv(const T* w, int64_t ldw, int n, const T* dinv, T* x, int6
   return RM_OK;
 }
 
-// The float32 block-Jacobi-scaled chain (PRE, 128-row blocks, tensor-core products) with its
-// blocks of the scaled triangle brought into shared memory by asynchronous copies, two blocks
-// ahead of the one being applied (a ring of three): a step's own time is then its product, not
-// the load latency of its block. Otherwise as trsv_chain_kernel<float, LOWER, false, 128, true>:
-// x_b = D_b^-1 y_b - sum_j pre_bj x_j, each x_j subtracted as it is released, in solve order;
-// pre holds full zero-padded 128 x 128 blocks (ld a multiple of 128), so every copy is in bounds.
+// The float32 block-Jacobi-scaled chain (PRE, 128-row blocks) with its blocks of the scaled
+// triangle brought into shared memory by asynchronous copies, two blocks ahead of the one being
+// applied (a ring of three): a step's own time is then its product, not the load latency of
+// its block. x_b = D_b^-1 y_b - sum_j pre_bj x_j, each x_j subtracted as it is released, in
+// solve order; pre holds full zero-padded 128 x 128 blocks (ld a multiple of 128), so every
+// copy is in bounds. The products are float32 FMAs on the CUDA cores: 128 x 128 x 16 per step
+// is 2^18 FMAs, about 2048 cycles of one SM's FP32 pipes, which beats three TF32 passes through
+// the warp-level tensor-core instructions (their rate is near the FMA rate) and, at 16
+// columns, tcgen05 too (an M = 128, K = 8 instruction costs the same at N = 16 as at N = 128).
+// Warp g owns rows 8 g .. 8 g + 7; lane (ks, cg) multiplies them by columns 8 cg .. 8 cg + 7 of
+// x over k = ks, ks + 16, ..., an 8 x 8 register tile, so that shared-memory reads (8 per k of
+// the block, 8 of x) take no more wavefronts than the FMAs take cycles. The partial sums stay in
+// registers from step to step; the sixteen K-slices of a warp sum them once, at the end.
 template <bool LOWER>
 __global__ void __launch_bounds__(kTB32 * 4)
     trsv_pre_ring_kernel(const float* __restrict__ pre, int64_t ldp, int n, const float* __restrict__ dinv, float* x,
                          int64_t ldx, int kc, int* flags, int* counter, unsigned* status) {
-  constexpr int TB = kTB32, THREADS = TB * 4, LDS = TB + 4, RING = 3, XS = 24;
+  constexpr int TB = kTB32, THREADS = TB * 4, LDS = TB + 4, RING = 3, NC = kKC, XS = NC + 4;
   extern __shared__ __align__(16) uint8_t smraw[];
   float(*ring)[TB][LDS] = reinterpret_cast<float(*)[TB][LDS]>(smraw);
-  float(*xs)[XS] = reinterpret_cast<float(*)[XS]>(smraw + (size_t)RING * TB * LDS * sizeof(float));
+  // x_j (times -1) or y_b, rows XS floats apart: the eight rows that one phase of a 16-byte load
+  // reads fall in eight different 16-byte bank groups (XS / 4 is odd)
+  float* xs = reinterpret_cast<float*>(smraw + (size_t)RING * TB * LDS * sizeof(float));
   __shared__ int ticket;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const int nblk = (n + TB - 1) / TB;
   if (tid == 0) ticket = atomicAdd(counter, 1);
   __syncthreads();
@@ -422,17 +431,13 @@ __global__ void __launch_bounds__(kTB32 * 4)
   const int b = LOWER ? t : nblk - 1 - t;
   const int r0 = b * TB, rows = min(TB, n - r0);
   auto dep = [&](int s) { return LOWER ? s : nblk - 1 - s; };  // the s-th block solved
-  const int g = lane >> 2, tq = lane & 3;
-  const int fr = 16 * (warp >> 1) + g, fc = 8 * (warp & 1) + 2 * tq;
-  auto prow = [&](int i) { return fr + 8 * (i >> 1); };
-  auto pcol = [&](int i) { return fc + (i & 1); };
+  const int lane = tid & 31, g = tid >> 5, ks = lane & 15, cg = lane >> 4;
 
-  float acc[4];
+  float acc[8][8];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = prow(i), c = pcol(i);
-    acc[i] = (r < rows && c < kc) ? x[(int64_t)(r0 + r) * ldx + c] : 0.0f;
-  }
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[i][c] = 0.0f;
   // item 0 is D_b^-1, item i >= 1 the block (b, dep(i - 1)); an item past t commits an empty
   // group, so that every thread counts the same groups
   auto issue = [&](int it) {
@@ -455,30 +460,34 @@ __global__ void __launch_bounds__(kTB32 * 4)
     }
     cp_async_commit();
   };
-  // a += sign * blk xs (this thread's fragment), 3xTF32 on the tensor cores
-  auto apply = [&](const float(*blk)[LDS], float sign) {
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 4
-    for (int k8 = 0; k8 < TB; k8 += 8) {
-      const float av[4] = {sign * blk[fr][k8 + tq], sign * blk[fr + 8][k8 + tq], sign * blk[fr][k8 + tq + 4],
-                           sign * blk[fr + 8][k8 + tq + 4]};
-      const float bv0 = xs[k8 + tq][8 * (warp & 1) + g], bv1 = xs[k8 + tq + 4][8 * (warp & 1) + g];
-      uint32_t ah[4], al[4];
+  // rows c0.. (cols of them valid) of x, times sign, into xs (zero past them and past kc)
+  auto put_x = [&](int c0, int cols, float sign) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        ah[i] = tc::to_tf32(av[i]);
-        al[i] = tc::to_tf32(av[i] - __uint_as_float(ah[i]));
-      }
-      const uint32_t bh0 = tc::to_tf32(bv0), bh1 = tc::to_tf32(bv1);
-      const uint32_t bl0 = tc::to_tf32(bv0 - __uint_as_float(bh0)), bl1 = tc::to_tf32(bv1 - __uint_as_float(bh1));
-      tc::mma_tf32_16x8x8(d, al, bh0, bh1);
-      tc::mma_tf32_16x8x8(d, ah, bl0, bl1);
-      tc::mma_tf32_16x8x8(d, ah, bh0, bh1);
+    for (int q = 0; q < TB * NC / THREADS; ++q) {
+      const int e = tid + q * THREADS, r = e / NC, c = e % NC;
+      xs[r * XS + c] = (r < cols && c < kc) ? sign * __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : 0.0f;
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) acc[i] += d[i];
   };
-  auto fetch = [&](int j) -> bool {  // wait for block j's release, then x_j into xs
+  // acc += blk xs over this thread's 8 x 8 tile and K-slice
+  auto apply = [&](const float(*blk)[LDS]) {
+#pragma unroll 2
+    for (int kk = 0; kk < TB / 16; ++kk) {
+      const int k = ks + 16 * kk;
+      float a[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = blk[8 * g + i][k];
+      const float4 x0 = *reinterpret_cast<const float4*>(xs + k * XS + 8 * cg);
+      const float4 x1 = *reinterpret_cast<const float4*>(xs + k * XS + 8 * cg + 4);
+      const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[i][c] = fmaf(a[i], xv[c], acc[i][c]);
+    }
+  };
+  // waits for block j's release, then -x_j into xs; the barrier also publishes the ring's
+  // copies that each thread waited for before it
+  auto fetch = [&](int j) -> bool {
     bool seen = ld_acquire(&flags[j]) != 0;
     if (!seen) {
       const uint64_t start = global_ns();
@@ -486,13 +495,7 @@ __global__ void __launch_bounds__(kTB32 * 4)
         if (global_ns() - start > kWaitLimitNs) break;
       }
     }
-    if (seen) {
-      const int c0 = j * TB, cols = min(TB, n - c0);
-      for (int e = tid; e < TB * kKC; e += THREADS) {
-        const int r = e / kKC, c = e % kKC;
-        xs[r][c] = (r < cols && c < kc) ? __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : 0.0f;
-      }
-    }
+    if (seen) put_x(j * TB, min(TB, n - j * TB), -1.0f);
     if (!__syncthreads_and(seen ? 1 : 0)) {
       if (tid == 0) flag_error(status, RM_DEV_TIMEOUT);
       return false;
@@ -503,33 +506,48 @@ __global__ void __launch_bounds__(kTB32 * 4)
   issue(0);
   issue(1);
   issue(2);
-  // z_b = D_b^-1 y_b
-#pragma unroll
-  for (int i = 0; i < 4; ++i) xs[prow(i)][pcol(i)] = acc[i];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) acc[i] = 0.0f;
-  cp_async_wait<2>();  // item 0 has landed
+  put_x(r0, rows, 1.0f);  // y_b
+  cp_async_wait<2>();     // item 0 has landed
   __syncthreads();
-  apply(ring[0], 1.0f);
+  apply(ring[0]);  // z_b = D_b^-1 y_b
   bool ok = true;
   for (int s = 0; s < t; ++s) {
     const int it = s + 1;
-    __syncthreads();  // the last apply's reads of its slot and of xs are done
-    issue(it + 2);    // into the slot of item it - 1, applied already
+    __syncthreads();     // the last apply's reads of its slot and of xs are done
+    issue(it + 2);       // into the slot of item it - 1, applied already
+    cp_async_wait<2>();  // item it has landed (it + 1 and it + 2 may be in flight)
     if (!fetch(dep(s))) {
       ok = false;
       break;
     }
-    cp_async_wait<2>();  // item it has landed (it + 1 and it + 2 may be in flight)
-    __syncthreads();
-    apply(ring[it % RING], -1.0f);
+    apply(ring[it % RING]);
   }
   cp_async_wait_all();  // no copy into shared memory outlives the CTA
-  if (ok) {
+  // the sixteen K-slices of a warp half (lanes ks = 0..15 of one cg) summed, halving the tile
+  // at each of four exchanges: rows by ks bits 3, 2, 1, then columns by bit 0. Lane ks ends with
+  // row 8 g + (ks >> 1) and columns 8 cg + 4 (ks & 1) .. + 3.
+  {
+    const bool b3 = ks & 8, b2 = ks & 4, b1 = ks & 2, b0 = ks & 1;
+    float v32[32], v16[16], v8[8], v4[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = prow(i), c = pcol(i);
-      if (r < rows && c < kc) x[(int64_t)(r0 + r) * ldx + c] = acc[i];
+    for (int j = 0; j < 32; ++j) {  // item j: row j / 8, column j % 8 of the kept half
+      const float lo = acc[j / 8][j % 8], hi = acc[4 + j / 8][j % 8];
+      v32[j] = (b3 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b3 ? lo : hi, 8);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      v16[j] = (b2 ? v32[16 + j] : v32[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v32[j] : v32[16 + j], 4);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      v8[j] = (b1 ? v16[8 + j] : v16[j]) + __shfl_xor_sync(0xffffffffu, b1 ? v16[j] : v16[8 + j], 2);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      v4[j] = (b0 ? v8[4 + j] : v8[j]) + __shfl_xor_sync(0xffffffffu, b0 ? v8[j] : v8[4 + j], 1);
+    const int r = 8 * g + (ks >> 1), c0 = 8 * cg + 4 * (ks & 1);
+    if (ok && r < rows) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (c0 + j < kc) x[(int64_t)(r0 + r) * ldx + c0 + j] = v4[j];
     }
   }
   // every thread's x is written before the barrier; thread 0's release store, ordered after it,
@@ -541,7 +559,7 @@ __global__ void __launch_bounds__(kTB32 * 4)
 template <bool LOWER>
 static int launch_trsv_pre_ring(const float* pre, int64_t ldp, int n, const float* dinv, float* x, int64_t ldx, int kc,
                                 int* flags, int* counter, unsigned* status, cudaStream_t stream) {
-  constexpr size_t smem = (size_t)3 * kTB32 * (kTB32 + 4) * sizeof(float) + (size_t)kTB32 * 24 * sizeof(float);
+  constexpr size_t smem = (size_t)3 * kTB32 * (kTB32 + 4) * sizeof(float) + (size_t)kTB32 * (kKC + 4) * sizeof(float);
   static bool set = false;
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(trsv_pre_ring_kernel<LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
