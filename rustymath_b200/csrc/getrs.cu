@@ -17,6 +17,7 @@ namespace rm {
 constexpr int kKC = kSolveCols;  // right-hand-side columns per launch
 constexpr int kTB64 = kSolveBlock;  // float64 block rows (64)
 constexpr int kTB32 = 128;          // float32 block rows
+constexpr int kPreKC = 8;           // columns per chain of the scaled float32 solve
 
 size_t diag_blocks_f64_bytes(int64_t n) { return diag_blocks_bytes_max(n); }
 
@@ -404,19 +405,25 @@ static int launch_trsv(const T* w, int64_t ldw, int n, const T* dinv, T* x, int6
 // applied (a ring of three): a step's own time is then its product, not the load latency of
 // its block. x_b = D_b^-1 y_b - sum_j pre_bj x_j, each x_j subtracted as it is released, in
 // solve order; pre holds full zero-padded 128 x 128 blocks (ld a multiple of 128), so every
-// copy is in bounds. The products are float32 FMAs on the CUDA cores: 128 x 128 x 16 per step
-// is 2^18 FMAs, about 2048 cycles of one SM's FP32 pipes, which beats three TF32 passes through
-// the warp-level tensor-core instructions (their rate is near the FMA rate) and, at 16
+// copy is in bounds. The products are float32 FMAs on the CUDA cores: 128 x 128 x 8 per step
+// is 2^17 FMAs, about 1024 cycles of one SM's FP32 pipes, which beats three TF32 passes through
+// the warp-level tensor-core instructions (their rate is near the FMA rate) and, at so few
 // columns, tcgen05 too (an M = 128, K = 8 instruction costs the same at N = 16 as at N = 128).
-// Warp g owns rows 8 g .. 8 g + 7; lane (ks, cg) multiplies them by columns 8 cg .. 8 cg + 7 of
-// x over k = ks, ks + 16, ..., an 8 x 8 register tile, so that shared-memory reads (8 per k of
-// the block, 8 of x) take no more wavefronts than the FMAs take cycles. The partial sums stay in
-// registers from step to step; the sixteen K-slices of a warp sum them once, at the end.
+// A launch runs one chain per kPreKC columns of x (blockIdx.y), each with its own tickets and
+// flags, so that the chains of a 16-column right-hand side run side by side on twice the SMs,
+// each step half the product and half the reduction. Lane (ks, h) of warp g multiplies rows
+// 4 (2 g + h) .. + 3 by the chunk's 8 columns of x over k = ks, ks + 16, ..., a 4 x 8 register
+// tile; the partial sums stay in registers from step to step, and the sixteen K-slices of a
+// warp half sum them once, at the end.
 template <bool LOWER>
 __global__ void __launch_bounds__(kTB32 * 4)
     trsv_pre_ring_kernel(const float* __restrict__ pre, int64_t ldp, int n, const float* __restrict__ dinv, float* x,
-                         int64_t ldx, int kc, int* flags, int* counter, unsigned* status) {
-  constexpr int TB = kTB32, THREADS = TB * 4, LDS = TB + 4, RING = 3, NC = kKC, XS = NC + 4;
+                         int64_t ldx, int k, int* flags, int* counter, int64_t chain_stride, unsigned* status) {
+  constexpr int TB = kTB32, THREADS = TB * 4, LDS = TB + 4, RING = 3, NC = kPreKC, XS = NC + 4;
+  x += (int64_t)blockIdx.y * NC;
+  flags += (int64_t)blockIdx.y * chain_stride;
+  counter += (int64_t)blockIdx.y * chain_stride;
+  const int kc = min(NC, k - (int)blockIdx.y * NC);
   extern __shared__ __align__(16) uint8_t smraw[];
   float(*ring)[TB][LDS] = reinterpret_cast<float(*)[TB][LDS]>(smraw);
   // x_j (times -1) or y_b, rows XS floats apart: the eight rows that one phase of a 16-byte load
@@ -431,13 +438,13 @@ __global__ void __launch_bounds__(kTB32 * 4)
   const int b = LOWER ? t : nblk - 1 - t;
   const int r0 = b * TB, rows = min(TB, n - r0);
   auto dep = [&](int s) { return LOWER ? s : nblk - 1 - s; };  // the s-th block solved
-  const int lane = tid & 31, g = tid >> 5, ks = lane & 15, cg = lane >> 4;
+  const int lane = tid & 31, ks = lane & 15, row0 = 4 * (tid >> 4);
 
-  float acc[8][8];
+  float acc[4][NC];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[i][c] = 0.0f;
+    for (int c = 0; c < NC; ++c) acc[i][c] = 0.0f;
   // item 0 is D_b^-1, item i >= 1 the block (b, dep(i - 1)); an item past t commits an empty
   // group, so that every thread counts the same groups
   auto issue = [&](int it) {
@@ -468,21 +475,21 @@ __global__ void __launch_bounds__(kTB32 * 4)
       xs[r * XS + c] = (r < cols && c < kc) ? sign * __ldcg(&x[(int64_t)(c0 + r) * ldx + c]) : 0.0f;
     }
   };
-  // acc += blk xs over this thread's 8 x 8 tile and K-slice
+  // acc += blk xs over this thread's 4 x 8 tile and K-slice
   auto apply = [&](const float(*blk)[LDS]) {
-#pragma unroll 2
+#pragma unroll 4
     for (int kk = 0; kk < TB / 16; ++kk) {
-      const int k = ks + 16 * kk;
-      float a[8];
+      const int kr = ks + 16 * kk;
+      float a[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = blk[8 * g + i][k];
-      const float4 x0 = *reinterpret_cast<const float4*>(xs + k * XS + 8 * cg);
-      const float4 x1 = *reinterpret_cast<const float4*>(xs + k * XS + 8 * cg + 4);
+      for (int i = 0; i < 4; ++i) a[i] = blk[row0 + i][kr];
+      const float4 x0 = *reinterpret_cast<const float4*>(xs + kr * XS);
+      const float4 x1 = *reinterpret_cast<const float4*>(xs + kr * XS + 4);
       const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[i][c] = fmaf(a[i], xv[c], acc[i][c]);
+        for (int c = 0; c < NC; ++c) acc[i][c] = fmaf(a[i], xv[c], acc[i][c]);
     }
   };
   // waits for block j's release, then -x_j into xs; the barrier also publishes the ring's
@@ -523,31 +530,31 @@ __global__ void __launch_bounds__(kTB32 * 4)
     apply(ring[it % RING]);
   }
   cp_async_wait_all();  // no copy into shared memory outlives the CTA
-  // the sixteen K-slices of a warp half (lanes ks = 0..15 of one cg) summed, halving the tile
-  // at each of four exchanges: rows by ks bits 3, 2, 1, then columns by bit 0. Lane ks ends with
-  // row 8 g + (ks >> 1) and columns 8 cg + 4 (ks & 1) .. + 3.
+  // the sixteen K-slices of a warp half (lanes ks = 0..15) summed, halving the tile at each of
+  // four exchanges: rows by ks bits 3 and 2, then columns by bits 1 and 0. Lane ks ends with row
+  // row0 + (ks >> 2) and columns 2 (ks & 3), 2 (ks & 3) + 1.
   {
     const bool b3 = ks & 8, b2 = ks & 4, b1 = ks & 2, b0 = ks & 1;
-    float v32[32], v16[16], v8[8], v4[4];
+    float v16[16], v8[8], v4[4], v2[2];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {  // item j: row j / 8, column j % 8 of the kept half
-      const float lo = acc[j / 8][j % 8], hi = acc[4 + j / 8][j % 8];
-      v32[j] = (b3 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b3 ? lo : hi, 8);
+    for (int j = 0; j < 16; ++j) {  // item j: row j / 8, column j % 8 of the kept half
+      const float lo = acc[j / 8][j % 8], hi = acc[2 + j / 8][j % 8];
+      v16[j] = (b3 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b3 ? lo : hi, 8);
     }
 #pragma unroll
-    for (int j = 0; j < 16; ++j)
-      v16[j] = (b2 ? v32[16 + j] : v32[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v32[j] : v32[16 + j], 4);
-#pragma unroll
     for (int j = 0; j < 8; ++j)
-      v8[j] = (b1 ? v16[8 + j] : v16[j]) + __shfl_xor_sync(0xffffffffu, b1 ? v16[j] : v16[8 + j], 2);
+      v8[j] = (b2 ? v16[8 + j] : v16[j]) + __shfl_xor_sync(0xffffffffu, b2 ? v16[j] : v16[8 + j], 4);
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-      v4[j] = (b0 ? v8[4 + j] : v8[j]) + __shfl_xor_sync(0xffffffffu, b0 ? v8[j] : v8[4 + j], 1);
-    const int r = 8 * g + (ks >> 1), c0 = 8 * cg + 4 * (ks & 1);
+      v4[j] = (b1 ? v8[4 + j] : v8[j]) + __shfl_xor_sync(0xffffffffu, b1 ? v8[j] : v8[4 + j], 2);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      v2[j] = (b0 ? v4[2 + j] : v4[j]) + __shfl_xor_sync(0xffffffffu, b0 ? v4[j] : v4[2 + j], 1);
+    const int r = row0 + (ks >> 2), c0 = 2 * (ks & 3);
     if (ok && r < rows) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (c0 + j < kc) x[(int64_t)(r0 + r) * ldx + c0 + j] = v4[j];
+      for (int j = 0; j < 2; ++j)
+        if (c0 + j < kc) x[(int64_t)(r0 + r) * ldx + c0 + j] = v2[j];
     }
   }
   // every thread's x is written before the barrier; thread 0's release store, ordered after it,
@@ -557,9 +564,9 @@ __global__ void __launch_bounds__(kTB32 * 4)
 }
 
 template <bool LOWER>
-static int launch_trsv_pre_ring(const float* pre, int64_t ldp, int n, const float* dinv, float* x, int64_t ldx, int kc,
-                                int* flags, int* counter, unsigned* status, cudaStream_t stream) {
-  constexpr size_t smem = (size_t)3 * kTB32 * (kTB32 + 4) * sizeof(float) + (size_t)kTB32 * (kKC + 4) * sizeof(float);
+static int launch_trsv_pre_ring(const float* pre, int64_t ldp, int n, const float* dinv, float* x, int64_t ldx, int k,
+                                int* flags, int* counter, int64_t chain_stride, unsigned* status, cudaStream_t stream) {
+  constexpr size_t smem = (size_t)3 * kTB32 * (kTB32 + 4) * sizeof(float) + (size_t)kTB32 * (kPreKC + 4) * sizeof(float);
   static bool set = false;
   if (!set) {
     RM_CUDA_TRY(cudaFuncSetAttribute(trsv_pre_ring_kernel<LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -567,8 +574,9 @@ static int launch_trsv_pre_ring(const float* pre, int64_t ldp, int n, const floa
     set = true;
   }
   const int nblk = (n + kTB32 - 1) / kTB32;
-  trsv_pre_ring_kernel<LOWER><<<nblk, kTB32 * 4, smem, stream>>>(pre, ldp, n, dinv, x, ldx, kc, flags, counter,
-                                                                   status);
+  const dim3 grid((unsigned)nblk, (unsigned)((k + kPreKC - 1) / kPreKC));
+  trsv_pre_ring_kernel<LOWER><<<grid, kTB32 * 4, smem, stream>>>(pre, ldp, n, dinv, x, ldx, k, flags, counter,
+                                                                   chain_stride, status);
   RM_LAUNCHED();
   return RM_OK;
 }
@@ -785,8 +793,9 @@ int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, f
   return RM_OK;
 }
 
+// flags and tickets of both chains per chunk of columns (chunks of kPreKC, the narrower kind)
 size_t trsv_f32_scratch_bytes(int64_t n, int64_t k) {
-  return (size_t)(2 * ((n + kTB32 - 1) / kTB32 + 1)) * sizeof(int) * (size_t)((k + kKC - 1) / kKC) + 256;
+  return (size_t)(2 * ((n + kTB32 - 1) / kTB32 + 1)) * sizeof(int) * (size_t)((k + kPreKC - 1) / kPreKC) + 256;
 }
 
 // x = U^-1 L^-1 x in place for the row-major float32 L\\U (unit L) of an LU whose row
@@ -796,19 +805,23 @@ int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv
                        int64_t ldx, int64_t k, void* scratch, unsigned* status, cudaStream_t stream) {
   if (n == 0 || k == 0) return RM_OK;
   const int nblk = (int)((n + kTB32 - 1) / kTB32);
-  const int chunks = (int)((k + kKC - 1) / kKC);
+  const int chunks = (int)((k + kKC - 1) / kKC), pre_chunks = (int)((k + kPreKC - 1) / kPreKC);
   int* flags = reinterpret_cast<int*>(scratch);
-  RM_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)(2 * (nblk + 1)) * sizeof(int) * chunks, stream));
+  const int64_t stride = 2 * (nblk + 1);  // ints per chunk: lower flags + ticket, upper flags + ticket
+  RM_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)stride * sizeof(int) * (pre ? pre_chunks : chunks), stream));
   const int64_t ldp = premultiplied_f32_ld(n);
+  if (pre) {
+    // every chunk of kPreKC columns in one launch per triangle, side by side
+    RM_TRY(launch_trsv_pre_ring<true>(pre, ldp, (int)n, dinv, x, ldx, (int)k, flags, flags + nblk, stride, status,
+                                      stream));
+    return launch_trsv_pre_ring<false>(pre, ldp, (int)n, dinv, x, ldx, (int)k, flags + nblk + 1, flags + 2 * nblk + 1,
+                                       stride, status, stream);
+  }
   for (int ch = 0; ch < chunks; ++ch) {
     const int kc = (int)std::min<int64_t>(kKC, k - (int64_t)ch * kKC);
-    int* f = flags + (size_t)ch * 2 * (nblk + 1);
+    int* f = flags + (size_t)ch * stride;
     float* xc = x + ch * kKC;
-    if (pre) {
-      RM_TRY(launch_trsv_pre_ring<true>(pre, ldp, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream));
-      RM_TRY(launch_trsv_pre_ring<false>(pre, ldp, (int)n, dinv, xc, ldx, kc, f + nblk + 1, f + 2 * nblk + 1, status,
-                                         stream));
-    } else {
+    {
       RM_TRY((launch_trsv<float, true, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream)));
       RM_TRY((launch_trsv<float, false, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f + nblk + 1,
                                                       f + 2 * nblk + 1, status, stream)));
