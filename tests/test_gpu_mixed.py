@@ -27,7 +27,8 @@ def rb():
 
 
 @pytest.mark.parametrize("n,k,kappa", [(1024, 16, 1e4), (1001, 3, 1e4), (130, 1, 1e3), (17, 2, 10.0), (5, 1, 2.0),
-                                       (2048, 5, 1e4), (1500, 17, 1e3), (1100, 17, 1e3)])
+                                       (2048, 5, 1e4), (1500, 17, 1e3), (1100, 17, 1e3), (1536, 16, 1e4),
+                                       (1200, 8, 1e3)])
 def test_mixed_meets_the_fp64_bar(rb, n, k, kappa):
     a, b = conditioned(n, k, kappa, n + k)
     x, reps = rb.solve_report(a, b, method="mixed")
