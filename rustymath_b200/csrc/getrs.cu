@@ -821,11 +821,9 @@ int lu_solve_f32_nopiv(const float* lu, int64_t ld, int64_t n, const float* dinv
     const int kc = (int)std::min<int64_t>(kKC, k - (int64_t)ch * kKC);
     int* f = flags + (size_t)ch * stride;
     float* xc = x + ch * kKC;
-    {
-      RM_TRY((launch_trsv<float, true, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream)));
-      RM_TRY((launch_trsv<float, false, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f + nblk + 1,
-                                                      f + 2 * nblk + 1, status, stream)));
-    }
+    RM_TRY((launch_trsv<float, true, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f, f + nblk, status, stream)));
+    RM_TRY((launch_trsv<float, false, false, kTB32>(lu, ld, (int)n, dinv, xc, ldx, kc, f + nblk + 1, f + 2 * nblk + 1,
+                                                    status, stream)));
   }
   return RM_OK;
 }
