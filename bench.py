@@ -186,6 +186,50 @@ def time_sgemm_update(torch, lib, dev, n, k=128, reps=10):
     return bytes_ / t / 1e9, t, bytes_, 3 * 2.0 * m * m * k / t / 1e12
 
 
+def time_cusolver(torch, a, b, reps=3):
+    """A comparison point, not part of the product path: torch.linalg.lu_factor + lu_solve
+    (cuSOLVER getrf/getrs) on the same float64 system, timed by CUDA events."""
+    prev = torch.backends.cuda.preferred_linalg_library()
+    torch.backends.cuda.preferred_linalg_library("cusolver")
+    try:
+        def go():
+            lu, piv = torch.linalg.lu_factor(a)
+            return torch.linalg.lu_solve(lu, piv, b)
+
+        go()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            xs = go()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        r = (b - a @ xs).abs().max().item()
+        berr = r / (a.abs().sum(1).max().item() * xs.abs().max().item() + b.abs().max().item())
+        return {"ms_per_solve": 1e3 * t, "solves_per_s": 1.0 / t, "backward_error": berr,
+                "what": "torch.linalg.lu_factor + lu_solve with the cuSOLVER backend (getrf + getrs), float64"}
+    finally:
+        torch.backends.cuda.preferred_linalg_library(prev)
+
+
+def parity_vs_oracle(a, b, x_oracle, arms, kappa):
+    """Each arm's solution against the oracle's (rustymath's lu_factor + lu_solve restated):
+    the normwise relative forward difference max_c ||x_c - xo_c||inf / ||xo_c||inf, and the
+    backward error of each from the oracle's double-double residual. The plain arm is held to
+    n eps, the others to kappa n eps."""
+    from oracle import oracle as O
+    n = a.shape[0]
+    eps = np.finfo(np.float64).eps
+    out = {"oracle_backward_error": O.backward_error(a, x_oracle, b), "kappa": kappa}
+    for name, x in arms.items():
+        fwd = float((np.abs(x - x_oracle).max(0) / np.abs(x_oracle).max(0)).max())
+        bound = n * eps if name == "plain_fp64" else kappa * n * eps
+        out[name] = {"forward_error_vs_oracle": fwd, "bound": bound, "within_bound": fwd <= bound,
+                     "backward_error_dd": O.backward_error(a, x, b)}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -309,8 +353,10 @@ def run_batched(args, rank, world, local):
         return plan, t, plan.results()[3], widths, int(launches)
 
     _, t_plain, rep_plain, w_plain, _ = arm("plain", max(1, min(args.steps, 3)))
+    x_plain = x.clone()
     clocks = ClockSampler(local)
     plan, t, rep, widths, launches = arm("mixed", args.steps, clocks)
+    x_mixed = x.clone()
     count = len(ns)
     # end to end: pinned host A, B -> device, the launch, X -> host, every step
     a_h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
@@ -348,7 +394,48 @@ def run_batched(args, rank, world, local):
             "gpu_launches": launches, "clocks": clocks.summary()}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_batched(ns, ks, a_h.numpy(), b_h.numpy(), 2000)
+        line["parity_vs_oracle"] = batch_parity(ns, ks, a_h.numpy(), b_h.numpy(),
+                                                {"plain_fp64": x_plain.cpu().numpy(), "mixed": x_mixed.cpu().numpy()},
+                                                sample=500)
     print(json.dumps(line), flush=True)
+
+
+def batch_parity(ns, ks, a_h, b_h, arms, sample, seed=0):
+    """A seeded sample of the batch against the oracle's solve, system by system: each arm's
+    normwise relative forward difference from the oracle's x; the plain arm held to n eps, the
+    mixed one to kappa_inf n eps (kappa of the sampled system, from NumPy)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    O.set_threads(1)
+    eps = np.finfo(np.float64).eps
+    a_off = np.concatenate([[0], np.cumsum(ns * ns)[:-1]])
+    b_off = np.concatenate([[0], np.cumsum(ns * ks)[:-1]])
+    idx = np.sort(np.random.default_rng(seed).choice(len(ns), min(sample, len(ns)), replace=False))
+
+    def one(i):
+        n, k = int(ns[i]), int(ks[i])
+        a = a_h[a_off[i]:a_off[i] + n * n].reshape(n, n)
+        b = b_h[b_off[i]:b_off[i] + n * k].reshape(n, k)
+        xo = O.solve(a, b)
+        kappa = float(np.linalg.cond(a, np.inf))
+        res = {}
+        for name, xs in arms.items():
+            x = xs[b_off[i]:b_off[i] + n * k].reshape(n, k)
+            fwd = float((np.abs(x - xo).max(0) / np.abs(xo).max(0)).max())
+            bound = n * eps if name == "plain_fp64" else kappa * n * eps
+            res[name] = (fwd, fwd / bound)
+        return res
+
+    with ThreadPoolExecutor(os.cpu_count()) as ex:
+        rows = list(ex.map(one, idx))
+    out = {"systems_checked": len(idx), "sample": f"{len(idx)} systems drawn by default_rng({seed})"}
+    for name in arms:
+        fwd = [r[name][0] for r in rows]
+        ratio = [r[name][1] for r in rows]
+        out[name] = {"max_forward_error_vs_oracle": max(fwd), "max_error_over_bound": max(ratio),
+                     "over_bound": int(sum(q > 1 for q in ratio)),
+                     "bound": "n eps" if name == "plain_fp64" else "kappa_inf n eps"}
+    return out
 
 
 ADJ_METRIC = "gradient solves/s: forward + adjoint (dA, db) of 4096 systems n=64 nrhs=2 on one B200"
@@ -477,6 +564,7 @@ def run_gemm(args, rank, world, local):
     clocks = ClockSampler(local)
     t_oz, e_oz, launches = timed(ozaki, steps, clocks)
     fl = 2.0 * n ** 3
+    cross = gemm_cross_check(torch, lib, dev) if not args.no_cpu_baseline else None
     line = {"metric": GEMM_METRIC, "value": fl / t_oz / 1e12, "unit": "TFLOP/s (FP64-equivalent)", "n_gpus": world,
             "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_oz, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int8 slices -> f64", "data": "synthetic",
@@ -485,8 +573,38 @@ def run_gemm(args, rank, world, local):
             "max_rel_error_vs_|A||B|": {"ozaki": e_oz, "native_fp64": e_nat, "cublas_fp64": e_cub},
             "native_fp64": {"tflops": fl / t_nat / 1e12, "ms": 1e3 * t_nat},
             "cublas_fp64": {"tflops": fl / t_cub / 1e12, "ms": 1e3 * t_cub},
+            "cross_check_2048_vs_oracle": cross,
             "gpu_launches": int(launches), "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
+
+
+def gemm_cross_check(torch, lib, dev, n=2048, seed=5):
+    """rm_dgemm and rm_dgemm_ozaki (8 slices) at n^3 against the oracle's product (rustymath's
+    PlusTimes.inner restated: packed 6 x 8 micro-kernel, in-order FMA), on the same wide-range
+    inputs (U(-1,1), rows of A and columns of B scaled by 10^U(-3,3), default_rng(seed)): the
+    largest difference of an item relative to (|A||B|)_ij, and the oracle's own time."""
+    from oracle import oracle as O
+    from rustymath_b200 import _lib
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-1, 1, (n, n)) * 10.0 ** rng.uniform(-3, 3, (n, 1))
+    b = rng.uniform(-1, 1, (n, n)) * 10.0 ** rng.uniform(-3, 3, (1, n))
+    O.set_threads(os.cpu_count())
+    t0 = time.perf_counter()
+    ref = O.dgemm(a, b)
+    t_cpu = time.perf_counter() - t0
+    mag = np.abs(a) @ np.abs(b)
+    ta, tb = torch.tensor(a, device=dev), torch.tensor(b, device=dev)
+    tc = torch.empty_like(ta)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {"n": n, "oracle_seconds": t_cpu, "oracle_threads": os.cpu_count(),
+           "what": "max_ij |C_ij - C_oracle_ij| / (|A||B|)_ij"}
+    _lib.check(lib.rm_dgemm(0, 0, n, n, n, 1.0, ta.data_ptr(), n, tb.data_ptr(), n, 0.0, tc.data_ptr(), n, sp), "dgemm")
+    out["native_fp64"] = float((np.abs(tc.cpu().numpy() - ref) / mag).max())
+    _lib.check(lib.rm_dgemm_ozaki(n, n, n, ta.data_ptr(), n, tb.data_ptr(), n, tc.data_ptr(), n, 8, sp), "ozaki")
+    out["ozaki_8_slices"] = float((np.abs(tc.cpu().numpy() - ref) / mag).max())
+    out["bound"] = n * np.finfo(np.float64).eps
+    out["within_bound"] = max(out["native_fp64"], out["ozaki_8_slices"]) <= out["bound"]
+    return out
 
 
 def run_small(args, rank, world, local):
@@ -647,8 +765,10 @@ def main():
     plain = {"solves_per_s": world * max(1, min(args.steps, 3)) / plain_t,
              "ms_per_solve": 1e3 * plain_t / max(1, min(args.steps, 3)), "backward_error": plain_rep.backward_error,
              "gpu_launches": int(plain_launches)}
+    x_plain = x.clone()
     clocks = ClockSampler(local)
     elapsed, rep, launches = timed(method, args.steps, args.warmup, clocks)
+    x_main = x.clone()
     value = world * args.steps / elapsed
     berr = rep.backward_error
     method_used = "plain FP64 LU" if rep.method_used == _lib.RM_METHOD_PLAIN_F64 else "FP32 LU + FP64 refinement"
@@ -703,9 +823,13 @@ def main():
                                         "frac": achieved / peak64,
                                         "peak_source": "cuBLAS FP64 GEMM 8192^3 in this run (no FP64 figure in "
                                                        "MEASURED_PEAKS.json)"}
-        cpu = None
+        cusolver = time_cusolver(torch, a, b)
+        cpu, parity = None, None
         if not args.no_cpu_baseline:
             cpu, x_cpu = cpu_baseline(a_h.numpy(), b_h.numpy())
+            parity = parity_vs_oracle(a_h.numpy(), b_h.numpy(), x_cpu,
+                                      {"plain_fp64": x_plain.cpu().numpy(), "headline": x_main.cpu().numpy()},
+                                      kappa=1e4)
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
                 "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["solves_per_s"],
                 "refinement_iterations": rep.iterations, "fell_back": rep.fell_back,
@@ -715,6 +839,9 @@ def main():
                 "config": {"workload": WORKLOAD, "method": method_used, "n": n, "nrhs": k,
                            "l2": "inputs larger than L2 (A is 512 MiB)", "parallelism": f"replicas x{world}"},
                 "backward_error": berr, "backward_error_target": n * 2.0 ** -53,
+                "parity_vs_oracle": parity, "cusolver_fp64": cusolver,
+                "speedup_vs_cusolver_fp64": value / cusolver["solves_per_s"],
+                "plain_vs_cusolver_time_ratio": plain["ms_per_solve"] / cusolver["ms_per_solve"],
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks.summary(), "tflops_lu": (2.0 / 3.0) * n ** 3 / (elapsed / args.steps) / 1e12 * world}
         print(json.dumps(line), flush=True)

@@ -78,6 +78,32 @@ int64_t rm_launch_count(void);
 /* Number of CUDA devices usable by this library (compute capability 10.x). */
 int rm_device_count(int *count);
 
+/* Errors that kernels find while they run (a row position outside 0..n-1 in a caller's perm,
+ * a bounded device-side wait that gave up) are recorded in a status word that each device
+ * holds. Entry points that synchronise read and clear it before they return. The asynchronous
+ * device forms (rm_dgemm, rm_dgemm_ozaki, rm_dlu_solve, rm_dlu_solve_noalloc, rm_dlu_factor
+ * without h_regular, rm_batch_plan_execute, rm_batch_plan_adjoint) cannot: their errors
+ * surface in the next call that reads the word.
+ * rm_take_status synchronises `stream`, then returns the recorded error as an rm status code
+ * (RM_BAD_ARG for a bad row position, RM_TIMEOUT for a wait) and clears the word. The word is
+ * per device, not per stream: an error of a call on another stream of the same device, still
+ * unread, is reported by whichever call reads the word first. */
+int rm_take_status(void *stream);
+
+/* ---- Test hooks. They make failures on the host, never on the GPU: no kernel faults, traps or
+ * hangs because of them. */
+#define RM_INJECT_OUT_OF_MEMORY 1 /* a scratch allocation reports device memory exhausted */
+#define RM_INJECT_CUDA_ERROR 2    /* a scratch allocation fails with a CUDA error */
+/* On the calling thread, after the next `after` events of `kind` succeed, `count` more fail
+ * as described; count 0 disarms. */
+int rm_test_inject_failure(int kind, int after, int count);
+/* Runs a small float64 triangular chain solve (n = 256, four 64-row blocks) whose first block
+ * row never runs, so the other blocks wait on a flag that nothing sets; every wait gives up
+ * after wait_ns nanoseconds (1000 <= wait_ns <= 2e9). Returns RM_TIMEOUT when the kernel
+ * reported its waits' expiry as it should (and RM_OK if it did not), on a status word of its
+ * own; synchronises. The device stays usable afterwards. */
+int rm_test_chain_timeout(int64_t wait_ns);
+
 /* C = alpha*op(A)*op(B) + beta*C, row-major, op(X) = X or X^T (trans* = RM_TRANS).
  * op(A) is m x k, op(B) is k x n, C is m x n. Mirrors Accelerated::xgemm
  * (core/src/linalg/accelerate.rs:211) with order fixed to row-major. */
@@ -118,14 +144,18 @@ int rm_dlu_solve_host(int64_t n, const double *h_factors, const int64_t *h_perm,
 /* rm_dlu_solve for callers that cannot allocate device memory during a call (a fixed
  * memory budget or arena that owns all device memory, a real-time loop kept away from the
  * allocator). It has no counterpart in the reference. Its scratch is a fixed __device__
- * array inside the library (about 4.7 MB, held on every GPU that loads the library until
- * the process exits), so it takes n <= RM_NOALLOC_MAX_N and k <= RM_NOALLOC_MAX_K and
+ * array inside the library of RM_NOALLOC_SCRATCH_BYTES (about 8.9 MB: the inverted 64 x 64
+ * diagonal blocks and couplings of a 4096-row factorization, 8 MiB, plus a permuted 4096 x 16
+ * right-hand side and the solve's flags), held on every GPU that loads the library until
+ * the process exits, so it takes n <= RM_NOALLOC_MAX_N and k <= RM_NOALLOC_MAX_K and
  * returns RM_BAD_ARG beyond them. The first call on a device looks the array up (once per
  * device); make that first call before any stream capture. All calls on one GPU share that
  * GPU's array and each leaves its contents for the next: calls that overlap on the same
- * GPU (on different streams) race on it, so the caller serialises them. */
+ * GPU (on different streams) race on it, so the caller serialises them. A bad row position
+ * in d_perm is reported through rm_take_status, as for rm_dlu_solve. */
 #define RM_NOALLOC_MAX_N 4096
 #define RM_NOALLOC_MAX_K 16
+#define RM_NOALLOC_SCRATCH_BYTES 8913672
 int rm_dlu_solve_noalloc(int64_t n, const double *d_factors, const int64_t *d_perm,
                          const double *d_b, int64_t k, double *d_x, int trans, void *stream);
 

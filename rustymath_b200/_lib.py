@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(HERE, "librm_cuda.so")
 RM_OK, RM_BAD_ARG, RM_NOT_REGULAR, RM_CUDA_ERROR = 0, 1, 2, 3
 RM_TIMEOUT, RM_NO_CONVERGENCE, RM_NO_DEVICE, RM_OUT_OF_MEMORY = 4, 5, 6, 7
 RM_METHOD_PLAIN_F64, RM_METHOD_F32_IR, RM_METHOD_GMRES_IR = 0, 1, 2
+RM_INJECT_OUT_OF_MEMORY, RM_INJECT_CUDA_ERROR = 1, 2
 
 _i32, _i64, _f64, _p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -40,6 +41,9 @@ SIGNATURES = {
     "rm_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "rm_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "rm_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    "rm_take_status": (ctypes.c_int, [_p]),
+    "rm_test_inject_failure": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "rm_test_chain_timeout": (ctypes.c_int, [_i64]),
     "rm_dgemm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _i64, _i64, _f64, _p, _i64, _p, _i64, _f64, _p,
                                 _i64, _p]),
     "rm_dgemm_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _i64, _i64, _f64, _p, _i64, _p, _i64, _f64,

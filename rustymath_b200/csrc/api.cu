@@ -5,7 +5,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -45,6 +47,23 @@ int device_sm_count() {
   return counts[dev];
 }
 
+int func_attribute(const void* kernel, cudaFuncAttribute attr, int value) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int>, int> done;  // (device, kernel, attribute) -> value
+  int dev = 0;
+  RM_CUDA_TRY(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(dev, kernel, (int)attr);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find(key);
+    if (it != done.end() && it->second == value) return RM_OK;
+  }
+  RM_CUDA_TRY(cudaFuncSetAttribute(kernel, attr, value));
+  std::lock_guard<std::mutex> lock(mu);
+  done[key] = value;
+  return RM_OK;
+}
+
 __device__ unsigned g_device_status;
 
 unsigned* device_status() {
@@ -82,21 +101,48 @@ int take_device_status(cudaStream_t stream) {
   return RM_OK;
 }
 
+// ------------------------------------------------------------------ failure injection (tests)
+// Per thread and RM_INJECT_* kind: how many events pass before the next failures, and how
+// many fail then.
+static thread_local int g_inject_after[3] = {0, 0, 0};
+static thread_local int g_inject_count[3] = {0, 0, 0};
+
+bool injected_failure(int kind) {
+  if (kind < 1 || kind > 2 || g_inject_count[kind] <= 0) return false;
+  if (g_inject_after[kind] > 0) {
+    --g_inject_after[kind];
+    return false;
+  }
+  --g_inject_count[kind];
+  return true;
+}
+
 // ------------------------------------------------------------------ scratch
 int scratch_alloc(void** p, size_t bytes, cudaStream_t stream) {
   *p = nullptr;
   if (bytes == 0) return RM_OK;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    // Keep freed scratch in the pool between calls instead of returning it to the driver.
+  if (injected_failure(RM_INJECT_CUDA_ERROR)) {
+    set_last_message("cudaMallocAsync failed (injected by rm_test_inject_failure)");
+    return RM_CUDA_ERROR;
+  }
+  {
+    // Keep freed scratch in each device's default pool between calls instead of returning it
+    // to the driver (once per device).
+    static std::mutex mu;
+    static std::vector<bool> pool_set;
     int dev = 0;
+    RM_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)pool_set.size() <= dev) pool_set.resize(dev + 1, false);
     cudaMemPool_t pool;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    if (!pool_set[dev] && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
       uint64_t threshold = UINT64_MAX;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+      pool_set[dev] = true;
     }
-  });
-  cudaError_t e = cudaMallocAsync(p, bytes, stream);
+  }
+  cudaError_t e = injected_failure(RM_INJECT_OUT_OF_MEMORY) ? cudaErrorMemoryAllocation
+                                                            : cudaMallocAsync(p, bytes, stream);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
     set_last_message("device memory exhausted");
@@ -269,6 +315,41 @@ int rm_last_error(char* buf, size_t len) {
   memcpy(buf, s.data(), n);
   buf[n] = 0;
   return RM_OK;
+}
+
+int rm_take_status(void* stream) {
+  RM_TRY(check_device());
+  return take_device_status(as_stream(stream));
+}
+
+int rm_test_inject_failure(int kind, int after, int count) {
+  if (kind < 1 || kind > 2 || after < 0 || count < 0) return RM_BAD_ARG;
+  g_inject_after[kind] = after;
+  g_inject_count[kind] = count;
+  return RM_OK;
+}
+
+int rm_test_chain_timeout(int64_t wait_ns) {
+  if (wait_ns < 1000 || wait_ns > 2000000000) return RM_BAD_ARG;
+  RM_TRY(check_device());
+  cudaStream_t s;
+  RM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st = RM_OK;
+  {
+    Scratch sc;
+    sc.stream = s;
+    st = scratch_alloc(&sc.base, chain_timeout_scratch_bytes(), s);
+    unsigned bits = 0;
+    if (st == RM_OK) st = chain_timeout_run((uint64_t)wait_ns, sc.base, &bits, s);
+    if (st == RM_OK) st = (bits & RM_DEV_TIMEOUT) ? RM_TIMEOUT : RM_OK;
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (st != RM_CUDA_ERROR && e != cudaSuccess) {
+    set_last_error(e, "stream synchronize", __FILE__, __LINE__);
+    st = RM_CUDA_ERROR;
+  }
+  cudaStreamDestroy(s);
+  return st;
 }
 
 int rm_device_count(int* count) {

@@ -911,14 +911,8 @@ static int plan_build(BatchPlan* p) {
   RM_CUDA_TRY(cudaMalloc(&p->d_flags, std::max<int64_t>(cnt, 1) * sizeof(int)));
   RM_CUDA_TRY(cudaMalloc(&p->d_counter, sizeof(int)));
   RM_CUDA_TRY(cudaMalloc(&p->d_w, p->w_bytes));
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(bt::batch_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(bt::Smem)));
-    RM_CUDA_TRY(cudaFuncSetAttribute(bt::batch_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(bt::Smem)));
-    set = true;
-  }
+  RM_TRY(smem_attribute(bt::batch_solve_kernel, sizeof(bt::Smem)));
+  RM_TRY(smem_attribute(bt::batch_adjoint_kernel, sizeof(bt::Smem)));
   int per_sm = 0;
   RM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bt::batch_solve_kernel, bt::THREADS,
                                                             sizeof(bt::Smem)));

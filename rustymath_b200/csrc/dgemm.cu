@@ -202,11 +202,7 @@ static int launch_cfg(const double* a, int64_t lda, const double* b, int64_t ldb
   } else {
     RM_TRY(make_tensor_map_2d(&tb, b, 8, k, n, ldb * 8, 16, C::BN, true));
   }
-  static bool configured = false;  // per template instance; the attribute call is idempotent
-  if (!configured) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(dgemm_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-    configured = true;
-  }
+  RM_TRY(smem_attribute(dgemm_kernel<C>, C::SMEM));
   dim3 grid((n + C::BN - 1) / C::BN, (m + C::BM - 1) / C::BM);
   dgemm_kernel<C><<<grid, C::THREADS, C::SMEM, stream>>>(ta, tb, c, ldc, m, n, k, alpha, beta, status);
   RM_LAUNCHED();

@@ -25,6 +25,9 @@
 // reciprocal unless the pivot is subnormal (factor.rs:506-508).
 #include <climits>
 
+#include <mutex>
+#include <vector>
+
 #include "rm_internal.h"
 
 namespace rm {
@@ -370,13 +373,13 @@ __global__ void __launch_bounds__(kSwapThreads)
 
 // The largest cluster (<= kMaxCluster CTAs of kPanelSmemBudget bytes) this device can place.
 template <typename T>
-static int panel_cluster_limit() {
-  static int limit = 0;
-  if (limit) return limit;
+static int find_panel_cluster_limit() {
+  int limit = 0;
   auto k = panel_kernel<T, true>;
-  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemBudget + 4096) != cudaSuccess ||
-      cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-      cudaFuncSetAttribute(panel_kernel<T, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+  if (smem_attribute(k, kPanelSmemBudget + 4096) != RM_OK ||
+      func_attribute(reinterpret_cast<const void*>(k), cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != RM_OK ||
+      func_attribute(reinterpret_cast<const void*>(panel_kernel<T, false>),
+                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != RM_OK) {
     cudaGetLastError();
     return limit = 8;
   }
@@ -398,6 +401,25 @@ static int panel_cluster_limit() {
   }
   return limit = 1;
 }
+
+// Found once per device (the attributes and the answer belong to that device).
+template <typename T>
+static int panel_cluster_limit() {
+  static std::mutex mu;
+  static std::vector<int> limits;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)limits.size() > dev && limits[dev]) return limits[dev];
+  }
+  const int limit = find_panel_cluster_limit<T>();
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)limits.size() <= dev) limits.resize(dev + 1, 0);
+  limits[dev] = limit;
+  return limit;
+}
+
 
 template <typename T>
 static int launch_panel(T* w, int64_t ldw, int n, int j0, int jb, int64_t* ipiv, cudaStream_t stream) {
@@ -556,12 +578,7 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
   // Look-ahead (n >= 1024): each trailing update does the next block's 128 columns first, on
   // the chain's stream; the rest runs on a side stream while the next block's leaves factor.
   // Only the block's row swaps on the columns right of it wait for that rest (it writes them).
-  static bool inv_set = false;
-  if (!inv_set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(invert_unit_lower_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kInv64Smem));
-    inv_set = true;
-  }
+  RM_TRY(smem_attribute(invert_unit_lower_f64_kernel, kInv64Smem));
   F64LookAhead la;
   const bool ahead = n >= 1024;
   cudaStream_t stream = caller;

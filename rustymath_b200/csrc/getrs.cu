@@ -126,14 +126,8 @@ template <typename T, bool COLMAJOR, int TB>
 static int launch_invert(const T* w, int64_t ldw, int64_t n, T* dinv, bool lower_unit, bool upper_unit,
                          cudaStream_t stream) {
   const size_t smem = (size_t)TB * (TB + 1) * sizeof(T);
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(invert_diag_blocks_kernel<T, COLMAJOR, TB>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    RM_CUDA_TRY(cudaFuncSetAttribute(coupling_kernel<T, COLMAJOR, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(2 * smem)));
-    set = true;
-  }
+  RM_TRY(smem_attribute(invert_diag_blocks_kernel<T, COLMAJOR, TB>, smem));
+  RM_TRY(smem_attribute(coupling_kernel<T, COLMAJOR, TB>, 2 * smem));
   dim3 grid((unsigned)((n + TB - 1) / TB), 2);
   invert_diag_blocks_kernel<T, COLMAJOR, TB><<<grid, TB, smem, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
   RM_LAUNCHED();
@@ -189,7 +183,7 @@ struct ChainLayout {
 template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE>
 __global__ void __launch_bounds__(TB * 4)
     trsv_chain_kernel(const T* __restrict__ w, int64_t ldw, int n, const T* __restrict__ dinv, T* x, int64_t ldx,
-                      int kc, int* flags, int* counter, unsigned* status) {
+                      int kc, int* flags, int* counter, unsigned* status, uint64_t wait_ns) {
   using Lay = ChainLayout<T, TB>;
   constexpr int THREADS = TB * 4;
   constexpr int LPT = TB * TB / THREADS;  // items of a block of T per thread
@@ -292,7 +286,7 @@ __global__ void __launch_bounds__(TB * 4)
     if (!seen) {
       const uint64_t start = global_ns();
       while (!(seen = ld_acquire(&flags[j]) != 0)) {
-        if (global_ns() - start > kWaitLimitNs) break;
+        if (global_ns() - start > wait_ns) break;
       }
     }
     if (seen) {
@@ -383,20 +377,54 @@ __global__ void __launch_bounds__(TB * 4)
   if (tid == 0) st_release(&flags[b], 1);
 }
 
+// Launches one chain (a CTA per block row). `ctas` < 0 launches all of them; the bounded-wait
+// self-test launches one fewer, having taken the first ticket itself.
 template <typename T, bool LOWER, bool COLMAJOR, int TB, bool PRE = false>
 static int launch_trsv(const T* w, int64_t ldw, int n, const T* dinv, T* x, int64_t ldx, int kc, int* flags,
-                       int* counter, unsigned* status, cudaStream_t stream) {
+                       int* counter, unsigned* status, cudaStream_t stream, uint64_t wait_ns = kWaitLimitNs,
+                       int ctas = -1) {
   const size_t smem = ChainLayout<T, TB>::bytes();
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    set = true;
-  }
+  RM_TRY(smem_attribute(trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE>, smem));
   const int nblk = (n + TB - 1) / TB;
-  trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE><<<nblk, TB * 4, smem, stream>>>(w, ldw, n, dinv, x, ldx, kc, flags,
-                                                                                  counter, status);
+  trsv_chain_kernel<T, LOWER, COLMAJOR, TB, PRE><<<ctas < 0 ? nblk : ctas, TB * 4, smem, stream>>>(
+      w, ldw, n, dinv, x, ldx, kc, flags, counter, status, wait_ns);
   RM_LAUNCHED();
+  return RM_OK;
+}
+
+// The bounded-wait self-test (rm_test_chain_timeout): a lower-triangular float64 chain at
+// n = 256 (four 64-row blocks, all zero: every load stays inside the buffers below) whose
+// ticket counter starts at 1, so block 0 never runs and never releases its flag. The three
+// CTAs launched (tickets 1..3, blocks 1..3, all resident at once) each wait on that flag, give
+// up after wait_ns, set RM_DEV_TIMEOUT in a status word of this call's own and return.
+namespace {
+constexpr int kTimeoutN = 256;
+struct TimeoutLayout {
+  static constexpr size_t w = 0;
+  static constexpr size_t dinv = w + (size_t)kTimeoutN * kTimeoutN * sizeof(double);
+  static constexpr size_t x = dinv + diag_blocks_bytes_max(kTimeoutN);
+  static constexpr size_t flags = x + (size_t)kTimeoutN * kKC * sizeof(double);
+  static constexpr size_t status = flags + 256;
+  static constexpr size_t total = status + 256;
+};
+}  // namespace
+
+size_t chain_timeout_scratch_bytes() { return TimeoutLayout::total; }
+
+int chain_timeout_run(uint64_t wait_ns, void* scratch, unsigned* bits, cudaStream_t stream) {
+  char* base = static_cast<char*>(scratch);
+  const int nblk = kTimeoutN / kTB64;
+  int* flags = reinterpret_cast<int*>(base + TimeoutLayout::flags);
+  unsigned* status = reinterpret_cast<unsigned*>(base + TimeoutLayout::status);
+  RM_CUDA_TRY(cudaMemsetAsync(scratch, 0, TimeoutLayout::total, stream));
+  const int first_ticket = 1;  // the counter sits after the nblk flags
+  RM_CUDA_TRY(cudaMemcpyAsync(flags + nblk, &first_ticket, sizeof(int), cudaMemcpyHostToDevice, stream));
+  RM_TRY((launch_trsv<double, true, false, kTB64>(
+      reinterpret_cast<const double*>(base + TimeoutLayout::w), kTimeoutN, kTimeoutN,
+      reinterpret_cast<const double*>(base + TimeoutLayout::dinv), reinterpret_cast<double*>(base + TimeoutLayout::x),
+      kKC, kKC, flags, flags + nblk, status, stream, wait_ns, nblk - 1)));
+  RM_CUDA_TRY(cudaMemcpyAsync(bits, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+  RM_CUDA_TRY(cudaStreamSynchronize(stream));
   return RM_OK;
 }
 
@@ -567,12 +595,7 @@ template <bool LOWER>
 static int launch_trsv_pre_ring(const float* pre, int64_t ldp, int n, const float* dinv, float* x, int64_t ldx, int k,
                                 int* flags, int* counter, int64_t chain_stride, unsigned* status, cudaStream_t stream) {
   constexpr size_t smem = (size_t)3 * kTB32 * (kTB32 + 4) * sizeof(float) + (size_t)kTB32 * (kPreKC + 4) * sizeof(float);
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(trsv_pre_ring_kernel<LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-    set = true;
-  }
+  RM_TRY(smem_attribute(trsv_pre_ring_kernel<LOWER>, smem));
   const int nblk = (n + kTB32 - 1) / kTB32;
   const dim3 grid((unsigned)nblk, (unsigned)((k + kPreKC - 1) / kPreKC));
   trsv_pre_ring_kernel<LOWER><<<grid, kTB32 * 4, smem, stream>>>(pre, ldp, n, dinv, x, ldx, k, flags, counter,
@@ -783,11 +806,7 @@ int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, f
   const int nblk = (int)((n + kTB32 - 1) / kTB32);
   if (nblk < 2) return RM_OK;
   const size_t smem = (size_t)kTB32 * (132 + 136) * sizeof(float);
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(premultiply_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    set = true;
-  }
+  RM_TRY(smem_attribute(premultiply_mma_kernel, smem));
   premultiply_mma_kernel<<<nblk * nblk, 256, smem, stream>>>(lu, ld, n, dinv, pre, premultiplied_f32_ld(n));
   RM_LAUNCHED();
   return RM_OK;

@@ -499,12 +499,8 @@ int getrf_lpp_f32(float* a, int64_t lda, int64_t n, int* perm, void* scratch, un
   float* l21lo = u12t + (size_t)n * kLppCols;  // rest x 128: low parts of L21 (ld 128) ...
   float* u12lo = l21lo + (size_t)n * kLppCols;  // ... and of U12^T, for the trailing update
   int* plocal = reinterpret_cast<int*>(u12lo + (size_t)n * kLppCols);
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(lpp_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLppSmem));
-    RM_CUDA_TRY(cudaFuncSetAttribute(lpp_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
-    set = true;
-  }
+  RM_TRY(smem_attribute(lpp_panel_kernel, kLppSmem));
+  RM_TRY(smem_attribute(lpp_post_kernel, kInvSmem));
   iota32_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 1024), 256, 0, stream>>>(perm, n);
   RM_LAUNCHED();
   // Look-ahead: the next panel's 128 columns of each trailing update go first, on `stream`;

@@ -18,6 +18,7 @@ namespace rm {
 // then the solve's permuted right-hand side and flags.
 constexpr size_t kNoallocBytes =
     ((diag_blocks_bytes_max(RM_NOALLOC_MAX_N) + 255) / 256) * 256 + getrs_scratch_bytes_max(RM_NOALLOC_MAX_N, RM_NOALLOC_MAX_K);
+static_assert(kNoallocBytes == RM_NOALLOC_SCRATCH_BYTES, "the header states the array's size");
 
 // Every GPU that loads this library holds this array until the process exits. All calls
 // share it; each call leaves its contents behind for the next.

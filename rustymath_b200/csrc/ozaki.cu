@@ -327,12 +327,7 @@ int dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double* a, int64_t lda, c
   int8_t* bsl = asl + (size_t)s * mp * kp;
   int* ea = reinterpret_cast<int*>(bsl + (size_t)s * np * kp);
   int* eb = ea + m;
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(oz::ozaki_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)oz::SMEM));
-    set = true;
-  }
+  RM_TRY(smem_attribute(oz::ozaki_order_kernel, oz::SMEM));
   const int mi = (int)m, ni = (int)n, ki = (int)k;
   // exponents and slices (the padding of the planes stays zero)
   RM_CUDA_TRY(cudaMemsetAsync(asl, 0, (size_t)s * (mp + np) * kp, stream));

@@ -191,4 +191,14 @@ int make_tensor_map_2d(CUtensorMap* map, const void* base, int elem_bytes, uint6
 
 int device_sm_count();
 
+// Sets a function attribute of `kernel` (cudaFuncSetAttribute) on the current device, once per
+// device and value: function attributes belong to one device's context, so a process that
+// drives several GPUs sets them on each. Safe to call from several threads.
+int func_attribute(const void* kernel, cudaFuncAttribute attr, int value);
+template <typename K>
+inline int smem_attribute(K* kernel, size_t bytes) {
+  return func_attribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        (int)bytes);
+}
+
 }  // namespace rm

@@ -176,6 +176,12 @@ int gmres_ir(const double* a, int64_t n, const double* b, int64_t k, double* x, 
 
 // ---------------------------------------------------------------- helpers (api.cu)
 int64_t round_up(int64_t x, int64_t m);
+// True (and counts it) when rm_test_inject_failure armed a failure of `kind` on this thread.
+bool injected_failure(int kind);
+// The bounded-wait self-test (getrs.cu): a float64 chain solve at n = 256 whose first block
+// never runs; the status bits its kernel set go to *bits (synchronises `stream`).
+size_t chain_timeout_scratch_bytes();
+int chain_timeout_run(uint64_t wait_ns, void* scratch, unsigned* bits, cudaStream_t stream);
 // Stream-ordered scratch allocation from the device's default pool.
 int scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
 void scratch_free(void* p, cudaStream_t stream);

@@ -464,12 +464,7 @@ template <int PASSES, bool TMA_EPI, bool LO_G = false>
 static int launch_sgemm(const CUtensorMap* maps, const SgemmPart& p1, const SgemmPart& p2, int n, int k, float alpha,
                         float beta, unsigned* status, cudaStream_t stream, int max_ctas) {
   using C = tc::Cfg<PASSES>;
-  static bool set = false;
-  if (!set) {
-    RM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tc_kernel<PASSES, TMA_EPI, LO_G>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-    set = true;
-  }
+  RM_TRY(smem_attribute(sgemm_tc_kernel<PASSES, TMA_EPI, LO_G>, C::SMEM));
   const int64_t tiles = (int64_t)p1.tiles + p2.tiles;
   const int ctas = max_ctas > 0 ? std::min(max_ctas, device_sm_count()) : device_sm_count();
   const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctas);

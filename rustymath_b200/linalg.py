@@ -342,6 +342,8 @@ def lu_solve(factors, p, b, trans=False):
         if device:
             st = lib.rm_dlu_solve(n, _ptr(f, True), _ptr(p, True), _ptr(b2, True), k, _ptr(x, True), int(trans),
                                   _stream(True))
+            if st == _lib.RM_OK:  # errors the kernels found (the device form is asynchronous)
+                st = lib.rm_take_status(_stream(True))
         else:
             st = lib.rm_dlu_solve_host(n, _ptr(f, False), _ptr(p, False), _ptr(b2, False), k, _ptr(x, False),
                                        int(trans))

@@ -79,3 +79,22 @@ def test_no_device_fails_loudly():
     c = ctypes.c_int(-1)
     from rustymath_b200 import _lib
     assert _lib.load().rm_device_count(ctypes.byref(c)) == 0 and c.value == 0
+
+
+def test_test_hooks_check_their_arguments(lib):
+    from rustymath_b200 import _lib
+    assert lib.rm_test_inject_failure(0, 0, 1) == _lib.RM_BAD_ARG
+    assert lib.rm_test_inject_failure(_lib.RM_INJECT_OUT_OF_MEMORY, -1, 1) == _lib.RM_BAD_ARG
+    assert lib.rm_test_inject_failure(_lib.RM_INJECT_CUDA_ERROR, 0, -1) == _lib.RM_BAD_ARG
+    assert lib.rm_test_inject_failure(_lib.RM_INJECT_CUDA_ERROR, 0, 0) == _lib.RM_OK
+    assert lib.rm_test_chain_timeout(10) == _lib.RM_BAD_ARG
+    assert lib.rm_test_chain_timeout(3_000_000_000) == _lib.RM_BAD_ARG
+
+
+def test_status_query_without_a_device(lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from rustymath_b200 import _lib
+    assert lib.rm_take_status(None) == _lib.RM_NO_DEVICE
+    assert lib.rm_test_chain_timeout(1_000_000) == _lib.RM_NO_DEVICE
