@@ -41,6 +41,7 @@ extern "C" {
 #define RM_NO_CONVERGENCE 5   /* refinement did not reach the tolerance and fallback was off */
 #define RM_NO_DEVICE 6        /* no CUDA device of compute capability 10.0 */
 #define RM_OUT_OF_MEMORY 7
+#define RM_NOT_POSITIVE_DEFINITE 8 /* a Cholesky pivot is not > 0: rustymath's cholesky gives None */
 
 #define RM_NO_TRANS 0
 #define RM_TRANS 1
@@ -141,6 +142,39 @@ int rm_dlu_solve(int64_t n, const double *d_factors, const int64_t *d_perm, cons
 int rm_dlu_solve_host(int64_t n, const double *h_factors, const int64_t *h_perm,
                       const double *h_b, int64_t k, double *h_x, int trans);
 
+/* LU of a stack of `count` n x n row-major matrices (n <= 256, back to back) in one launch:
+ * each matrix's factors (column-major) and row positions as rm_dlu_factor gives them, one CTA
+ * per matrix; d_regular[i] (optional) as LuWork::regular. Stacked::lu (src/linalg/stacked.rs:
+ * 174-187). Partial pivoting by the greatest magnitude, NaN never chosen; among equal
+ * magnitudes the lowest row of the input, where rustymath takes the first in its current
+ * (already swapped) row order. Asynchronous. */
+int rm_dlu_factor_batched(int64_t count, int64_t n, const double *d_a, double *d_factors, int64_t *d_perm,
+                          int32_t *d_regular, void *stream);
+
+/* The inverse of the matrix that the factors and perm describe: d_out = A^-1, row-major n x n,
+ * as Lu::inverse (core/src/linalg/factor.rs:150-154; lu_inverse, factor.rs:645-664): U^-1 L^-1
+ * from the identity, 16 columns at a time, the lower solve of each group of columns starting
+ * at the block row of its first column (L^-1 is zero above its diagonal), then the columns
+ * permuted by perm. Asynchronous; a bad row position surfaces through rm_take_status. */
+int rm_dlu_inverse(int64_t n, const double *d_factors, const int64_t *d_perm, double *d_out, void *stream);
+int rm_dlu_inverse_host(int64_t n, const double *h_factors, const int64_t *h_perm, double *h_out);
+
+/* Determinants of a stack of `count` factorizations (n x n column-major factors and n row
+ * positions each, back to back): d_det[i] as Lu::determinant (factor.rs:174-176: U's diagonal
+ * multiplied in order from 1, negated when perm is odd; odd(), factor.rs:186-194) and d_sign[i],
+ * d_logabs[i] as Lu::log_determinant (factor.rs:177-183: sign 0 and log -inf once a diagonal
+ * item is 0). Any output may be NULL. The stack forms of Stacked::det and slogdet
+ * (src/linalg/stacked.rs:136-171) factor first. Asynchronous. */
+int rm_dlu_determinant(int64_t count, int64_t n, const double *d_factors, const int64_t *d_perm,
+                       double *d_det, double *d_sign, double *d_logabs, void *stream);
+
+/* x = A^-1 b (A^-T b when trans) for each of a stack of `count` factorizations with n <= 256
+ * (column-major factors and row positions back to back) and n x k right-hand sides (k <= 64,
+ * row-major, back to back), one launch: Stacked::lu_solve (src/linalg/stacked.rs:190-204).
+ * b and x may alias. Asynchronous; a bad row position surfaces through rm_take_status. */
+int rm_dlu_solve_batched(int64_t count, int64_t n, const double *d_factors, const int64_t *d_perm,
+                         const double *d_b, int64_t k, double *d_x, int trans, void *stream);
+
 /* rm_dlu_solve for callers that cannot allocate device memory during a call (a fixed
  * memory budget or arena that owns all device memory, a real-time loop kept away from the
  * allocator). It has no counterpart in the reference. Its scratch is a fixed __device__
@@ -197,6 +231,25 @@ int rm_dgemm_ozaki(int64_t m, int64_t n, int64_t k, const double *d_a, int64_t l
                    int64_t ldb, double *d_c, int64_t ldc, int slices, void *stream);
 int rm_dgemm_ozaki_host(int64_t m, int64_t n, int64_t k, const double *h_a, int64_t lda, const double *h_b,
                         int64_t ldb, double *h_c, int64_t ldc, int slices);
+
+/* ---- Cholesky.
+ * L with L L^T = A for the symmetric positive definite n x n row-major A, reading only A's
+ * lower triangle; L is row-major with zeros above the diagonal. Mirrors rustymath's cholesky
+ * (core/src/linalg/factor.rs:267; cholesky_factor, factor.rs:750-795). Synchronises on
+ * `stream`; returns RM_NOT_POSITIVE_DEFINITE where rustymath gives None (a pivot that is not
+ * > 0, NaN included), d_l then unspecified. */
+int rm_dcholesky(int64_t n, const double *d_a, double *d_l, void *stream);
+int rm_dcholesky_host(int64_t n, const double *h_a, double *h_l);
+/* A stack of `count` n x n matrices (n <= 128) back to back, in one launch: each L as
+ * rm_dcholesky gives it, or NaN in every item where that matrix is not positive definite, as
+ * rustymath's stack form (src/linalg/stacked.rs:259-268); d_ok[i] (optional) is 1 or 0.
+ * Asynchronous on `stream`. */
+int rm_dcholesky_batched(int64_t count, int64_t n, const double *d_a, double *d_l, int32_t *d_ok,
+                         void *stream);
+/* x = A^-1 b from A's Cholesky factor L (L y = b, then L^T x = y, the triangular solves of
+ * rm_dtrsm); b and x n x k row-major, and they may alias. Synchronises. */
+int rm_dcholesky_solve(int64_t n, const double *d_l, const double *d_b, int64_t k, double *d_x,
+                       void *stream);
 
 /* ---- Batched solves: many small systems of uneven size in one persistent launch.
  * System i is the n[i] x n[i] row-major float64 A at d_a + a_off[i] (items), its right-hand

@@ -38,6 +38,7 @@ def _load():
         "ora_lu_determinant": (_f64, [_i64, _p, _p]),
         "ora_lu_log_determinant": (None, [_i64, _p, _p, _p, _p]),
         "ora_regular": (ctypes.c_int, [_i64, _p, _p]),
+        "ora_cholesky": (ctypes.c_int, [_i64, _p, _p]),
         "ora_solve": (ctypes.c_int, [_i64, _p, _p, _i64, _p]),
         "ora_backward_error": (_f64, [_i64, _p, _p, _p, _i64]),
         "ora_residual_dd": (None, [_i64, _p, _p, _p, _i64, _p]),
@@ -156,6 +157,16 @@ def lu_log_determinant(factors, perm):
     s, l = ctypes.c_double(), ctypes.c_double()
     lib().ora_lu_log_determinant(f.shape[0], _ptr(f), _ptr(p), ctypes.addressof(s), ctypes.addressof(l))
     return s.value, l.value
+
+
+def cholesky(a):
+    """L with L L^T = A (row-major, zeros above the diagonal), or None where A is not positive
+    definite: rustymath's cholesky (core/src/linalg/factor.rs:750-795)."""
+    a = _c(a)
+    n = a.shape[0]
+    out = np.zeros((n, n))
+    ok = lib().ora_cholesky(n, _ptr(a), _ptr(out))
+    return out if ok else None
 
 
 def regular(a, factors):

@@ -489,6 +489,73 @@ void ora_lu_log_determinant(int64_t n, const double *factors, const int64_t *per
     *logabs = l;
 }
 
+/* ---------------------------------------------------------------- Cholesky */
+
+/* cholesky_panel (factor.rs:750-773): factors columns c0..c1 of the rows-row block that
+ * `panel` holds column by column (columns ld apart), halving the columns above LEAF; a leaf
+ * column takes d = sqrt(its diagonal), divides the items below by d (divide: the reciprocal
+ * unless d is subnormal) and removes itself from the leaf's later columns by axpy. 0 where
+ * a diagonal is not > 0 (not positive definite; NaN too). */
+static int cholesky_panel(double *panel, int64_t rows, int64_t ld, int64_t c0, int64_t c1) {
+    if (c1 - c0 > LEAF) {
+        int64_t mid = (c0 + c1) / 2;
+        if (!cholesky_panel(panel, rows, ld, c0, mid)) return 0;
+        /* columns mid..c1, rows mid..: -= L(rows, c0..mid) L(cols, c0..mid)^T */
+        view l = vrows(panel + c0 * ld + mid, ld);
+        gemm_v(panel + mid * ld + mid, ld, vtr(l), l, c1 - mid, mid - c0, rows - mid, -1.0, 1.0);
+        return cholesky_panel(panel, rows, ld, mid, c1);
+    }
+    for (int64_t c = c0; c < c1; c++) {
+        double d = panel[c * ld + c];
+        if (!(d > 0.0)) return 0;
+        d = sqrt(d);
+        panel[c * ld + c] = d;
+        double *lc = panel + c * ld + c + 1;
+        divide(lc, rows - c - 1, d);
+        for (int64_t j = 0; j < c1 - c - 1; j++) {
+            double *column = panel + (c + 1 + j) * ld;
+            axpy(column + c + 1 + j, -lc[j], lc + j, rows - c - 1 - j);
+        }
+    }
+    return 1;
+}
+
+/* cholesky_factor (factor.rs:776-795): blocks of cholesky_block(n) = clamp(n/8, 32, 128)
+ * columns (factor.rs:29) in a copy with rows stride(n) apart; each block's columns factor in
+ * a transposed copy (columns stride(rows) apart), go back, and `gram` (linalg.rs:777-779, the
+ * lower triangle of C - X X^T) updates the rest. L row-major with zeros above the diagonal;
+ * 0 (nothing written) where the matrix is not positive definite. Only a's lower triangle is
+ * read. gram computes only the lower triangle; here the whole product is formed, whose lower
+ * triangle has the same bits (every item folds its k terms in order on its own). */
+int ora_cholesky(int64_t n, const double *a, double *out) {
+    if (n == 0) return 1;
+    int64_t ld = stride_of(n);
+    double *l = calloc((size_t)(n * ld), sizeof(double));
+    for (int64_t i = 0; i < n; i++) memcpy(l + i * ld, a + i * n, (size_t)n * sizeof(double));
+    int64_t width = n / 8 < 32 ? 32 : (n / 8 > 128 ? 128 : n / 8);
+    int64_t pl0 = stride_of(n);
+    double *panel = malloc((size_t)(pl0 * width) * sizeof(double));
+    int ok = 1;
+    for (int64_t k0 = 0; k0 < n; k0 += width) {
+        int64_t k1 = k0 + width < n ? k0 + width : n;
+        int64_t nb = k1 - k0, rows = n - k0, w = n - k1, pl = stride_of(rows);
+        for (int64_t j = 0; j < nb; j++)
+            for (int64_t i = 0; i < rows; i++) panel[j * pl + i] = l[(k0 + i) * ld + k0 + j];
+        if (!cholesky_panel(panel, rows, pl, 0, nb)) { ok = 0; break; }
+        for (int64_t i = 0; i < rows; i++)
+            for (int64_t j = 0; j < nb; j++) l[(k0 + i) * ld + k0 + j] = panel[j * pl + i];
+        if (w == 0) break;
+        view x = vtr(vrows(panel + nb, pl));
+        gemm_v(l + k1 * ld + k1, ld, x, vtr(x), w, nb, w, -1.0, 1.0);
+    }
+    if (ok)
+        for (int64_t i = 0; i < n; i++)
+            for (int64_t j = 0; j < n; j++) out[i * n + j] = j <= i ? l[i * ld + j] : 0.0;
+    free(panel);
+    free(l);
+    return ok;
+}
+
 int ora_regular(int64_t n, const double *a, const double *factors) {
     if (n == 0) return 0;
     double top = greatest_abs(a, n * n, 1);

@@ -59,6 +59,11 @@ void ora_lu_log_determinant(int64_t n, const double *factors, const int64_t *per
                             double *sign, double *logabs);
 
 /* LuWork::regular (factor.rs:221-226): 1 when every |u_ii| > eps*n*max|a|. */
+/* L (row-major, zeros above the diagonal) with L L^T = A from A's lower triangle, as
+ * rustymath's cholesky (core/src/linalg/factor.rs:750-795); 0 where A is not positive
+ * definite (out untouched). */
+int ora_cholesky(int64_t n, const double *a, double *out);
+
 int ora_regular(int64_t n, const double *a, const double *factors);
 
 /* solve (factor.rs:279) for a square, regular a: returns 0 and writes x, or returns 1

@@ -10,6 +10,7 @@ LIB_PATH = os.path.join(HERE, "librm_cuda.so")
 
 RM_OK, RM_BAD_ARG, RM_NOT_REGULAR, RM_CUDA_ERROR = 0, 1, 2, 3
 RM_TIMEOUT, RM_NO_CONVERGENCE, RM_NO_DEVICE, RM_OUT_OF_MEMORY = 4, 5, 6, 7
+RM_NOT_POSITIVE_DEFINITE = 8
 RM_METHOD_PLAIN_F64, RM_METHOD_F32_IR, RM_METHOD_GMRES_IR = 0, 1, 2
 RM_INJECT_OUT_OF_MEMORY, RM_INJECT_CUDA_ERROR = 1, 2
 
@@ -76,6 +77,15 @@ SIGNATURES = {
     "rm_dgemm_ozaki": (ctypes.c_int, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, ctypes.c_int, _p]),
     "rm_batch_plan_adjoint_results": (ctypes.c_int, [_p, _p, _p]),
     "rm_batch_plan_destroy": (ctypes.c_int, [_p]),
+    "rm_dlu_factor_batched": (ctypes.c_int, [_i64, _i64, _p, _p, _p, _p, _p]),
+    "rm_dlu_inverse": (ctypes.c_int, [_i64, _p, _p, _p, _p]),
+    "rm_dlu_inverse_host": (ctypes.c_int, [_i64, _p, _p, _p]),
+    "rm_dlu_determinant": (ctypes.c_int, [_i64, _i64, _p, _p, _p, _p, _p, _p]),
+    "rm_dlu_solve_batched": (ctypes.c_int, [_i64, _i64, _p, _p, _p, _i64, _p, ctypes.c_int, _p]),
+    "rm_dcholesky": (ctypes.c_int, [_i64, _p, _p, _p]),
+    "rm_dcholesky_host": (ctypes.c_int, [_i64, _p, _p]),
+    "rm_dcholesky_batched": (ctypes.c_int, [_i64, _i64, _p, _p, _p, _p]),
+    "rm_dcholesky_solve": (ctypes.c_int, [_i64, _p, _p, _i64, _p, _p]),
     "rm_dsolve_batched": (ctypes.c_int, [_i64, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.POINTER(SolveOptions),
                                          ctypes.POINTER(BatchReport), _p]),
 }
@@ -87,6 +97,10 @@ class RmError(RuntimeError):
     def __init__(self, status, message):
         super().__init__(message)
         self.status = status
+
+
+class NotPositiveDefinite(ValueError):
+    """A Cholesky pivot is not > 0: rustymath's cholesky gives None here (and its stacks NaN)."""
 
 
 class NotRegular(ValueError):
@@ -128,4 +142,6 @@ def check(status, what):
         raise ValueError(msg)
     if status == RM_NOT_REGULAR:
         raise NotRegular(msg)
+    if status == RM_NOT_POSITIVE_DEFINITE:
+        raise NotPositiveDefinite(msg)
     raise RmError(status, msg)

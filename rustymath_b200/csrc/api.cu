@@ -304,6 +304,7 @@ const char* rm_status_string(int status) {
     case RM_NO_CONVERGENCE: return "refinement did not converge";
     case RM_NO_DEVICE: return "no compute capability 10.x device";
     case RM_OUT_OF_MEMORY: return "out of device memory";
+    case RM_NOT_POSITIVE_DEFINITE: return "matrix not positive definite (a Cholesky pivot is not > 0)";
     default: return "unknown status";
   }
 }

@@ -825,6 +825,52 @@ __global__ void __launch_bounds__(THREADS, 2) batch_adjoint_kernel(Adjoint aj) {
   }
 }
 
+// Stacked::lu (src/linalg/stacked.rs:174-187) in one launch: matrix blockIdx.x of a stack of
+// n x n row-major matrices (n <= NMAX, back to back) factored in float64 by bfactor in its own
+// slice of wbuf (w_stride bytes apart), then written in rustymath's layout: factors column-
+// major, (L U)(i, j) = W[piv[i]][j] at factors[j*n + i] (coalesced over i), perm[i] = piv[i];
+// regular[m] (when not NULL) as LuWork::regular (factor.rs:221-226): every |u_ii| > eps n
+// max|a|, max ignoring NaN, a NaN pivot counting as regular.
+__global__ void __launch_bounds__(THREADS) batch_factor_kernel(const double* __restrict__ a, int n,
+                                                               unsigned char* wbuf, int64_t w_stride,
+                                                               double* __restrict__ factors, int64_t* __restrict__ perm,
+                                                               int32_t* regular) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  Smem& sm = *reinterpret_cast<Smem*>(dsm);
+  __shared__ int irregular;
+  const int64_t m = blockIdx.x;
+  const int ld = (n + 3) & ~3;
+  double* W = reinterpret_cast<double*>(wbuf + m * w_stride);
+  const double* am = a + m * n * n;
+  load_w<double>(am, n, W, ld);
+  if (threadIdx.x == 0) {
+    sm.zero_pivot = 0;
+    irregular = 0;
+  }
+  __syncthreads();
+  int my_pos = -1;
+  bfactor<double, 16>(W, ld, n, sm, my_pos);
+  double* fm = factors + m * n * n;
+  for (int e = threadIdx.x; e < n * n; e += THREADS) {
+    const int j = e / n, i = e - j * n;
+    fm[e] = W[(int64_t)sm.piv[i] * ld + j];
+  }
+  for (int i = threadIdx.x; i < n; i += THREADS) perm[m * n + i] = sm.piv[i];
+  if (regular) {
+    double amax = 0.0;
+    for (int e = threadIdx.x; e < n * n; e += THREADS) amax = fmax(amax, fabs(am[e]));
+#pragma unroll
+    for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+    if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5][0] = amax;
+    __syncthreads();
+    double big = 0.0;
+    for (int q = 0; q < WARPS; ++q) big = fmax(big, sm.red[q][0]);
+    if (my_pos >= 0 && fabs(W[(int64_t)threadIdx.x * ld + my_pos]) <= DBL_EPSILON * n * big) atomicOr(&irregular, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) regular[m] = irregular ? 0 : 1;
+  }
+}
+
 }  // namespace bt
 
 // ------------------------------------------------------------------ the plan (host)
@@ -938,14 +984,16 @@ static bt::Batch batch_args(BatchPlan* p, const double* a, const double* b, doub
   return q;
 }
 
-// the counter reset and the one persistent launch, over items [first, last)
+// the counter reset and the one persistent launch, over items [first, last); a launch being
+// captured into the plan's graph is counted when the graph runs, not here
 static int launch_batch(BatchPlan* p, const double* a, const double* b, double* x, int first, int last,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool captured = false) {
   RM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, sizeof(int), s));
   const int items = last - first;
   const int grid = std::min(p->grid, std::max(items, 1));
   bt::batch_solve_kernel<<<grid, bt::THREADS, sizeof(bt::Smem), s>>>(batch_args(p, a, b, x, first, last));
-  RM_LAUNCHED();
+  if (!captured) note_launch();
+  RM_CUDA_TRY(cudaGetLastError());
   return RM_OK;
 }
 
@@ -991,7 +1039,7 @@ int batch_plan_execute(BatchPlan* p, const double* a, const double* b, double* x
     }
     cudaGraph_t g = nullptr;
     RM_CUDA_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-    const int st = launch_batch(p, a, b, x, 0, (int)p->count, p->stream);
+    const int st = launch_batch(p, a, b, x, 0, (int)p->count, p->stream, true);
     const cudaError_t e = cudaStreamEndCapture(p->stream, &g);
     if (st != RM_OK) {
       if (g) cudaGraphDestroy(g);
@@ -1180,6 +1228,34 @@ int rm_batch_plan_destroy(rm_batch_plan* plan) {
   if (!plan) return RM_OK;
   rm::batch_plan_destroy(plan->p);
   delete plan;
+  return RM_OK;
+}
+
+int rm_dlu_factor_batched(int64_t count, int64_t n, const double* d_a, double* d_factors, int64_t* d_perm,
+                          int32_t* d_regular, void* stream) {
+  if (count < 0 || n < 0 || n > rm::bt::NMAX || (count > 0 && n > 0 && (!d_a || !d_factors || !d_perm)))
+    return RM_BAD_ARG;
+  if (count == 0 || n == 0) return RM_OK;
+  RM_TRY(rm::check_device());
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t ld = (n + 3) & ~3;
+  const int64_t stride = (n * ld * 8 + 255) / 256 * 256;
+  RM_TRY(rm::smem_attribute(rm::bt::batch_factor_kernel, sizeof(rm::bt::Smem)));
+  for (int64_t first = 0; first < count; first += 65536) {
+    const int64_t c = std::min<int64_t>(count - first, 65536);
+    void* w = nullptr;
+    RM_TRY(rm::scratch_alloc(&w, (size_t)(c * stride), s));
+    rm::bt::batch_factor_kernel<<<(unsigned)c, rm::bt::THREADS, sizeof(rm::bt::Smem), s>>>(
+        d_a + first * n * n, (int)n, static_cast<unsigned char*>(w), stride, d_factors + first * n * n,
+        d_perm + first * n, d_regular ? d_regular + first : nullptr);
+    const cudaError_t e = cudaGetLastError();
+    rm::scratch_free(w, s);
+    rm::note_launch();
+    if (e != cudaSuccess) {
+      rm::set_last_error(e, "batch_factor_kernel", __FILE__, __LINE__);
+      return RM_CUDA_ERROR;
+    }
+  }
   return RM_OK;
 }
 

@@ -623,6 +623,16 @@ __global__ void permute_rows_kernel(const double* __restrict__ b, int64_t ldb, c
   }
 }
 
+int trsv_chain_f64(bool lower, bool colmajor, const double* w, int64_t ldw, int n, const double* dinv, double* x,
+                   int64_t ldx, int kc, int* flags, int* counter, unsigned* status, cudaStream_t stream) {
+  if (lower && colmajor)
+    return launch_trsv<double, true, true, kTB64>(w, ldw, n, dinv, x, ldx, kc, flags, counter, status, stream);
+  if (lower) return launch_trsv<double, true, false, kTB64>(w, ldw, n, dinv, x, ldx, kc, flags, counter, status, stream);
+  if (colmajor)
+    return launch_trsv<double, false, true, kTB64>(w, ldw, n, dinv, x, ldx, kc, flags, counter, status, stream);
+  return launch_trsv<double, false, false, kTB64>(w, ldw, n, dinv, x, ldx, kc, flags, counter, status, stream);
+}
+
 size_t getrs_f64_scratch_bytes(int64_t n, int64_t k) { return getrs_scratch_bytes_max(n, k); }
 
 int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const int64_t* perm, const double* dinv,

@@ -91,6 +91,12 @@ int getrs_f64(const double* lu, int64_t ld, bool lu_colmajor, int64_t n, const i
               const double* b, int64_t ldb, int64_t k, double* x, int64_t ldx, void* scratch, unsigned* status,
               cudaStream_t stream, bool trans = false);
 size_t diag_blocks_f64_bytes(int64_t n);
+// One float64 block-chained triangular solve (a CTA per kSolveBlock-row block) of kc <= kSolveCols
+// columns of x in place: the lower or upper triangle of T, T(i, j) at w[i*ldw + j] (w[j*ldw + i]
+// when colmajor), with the diagonal-block inverses of invert_diag_blocks_f64; flags[nblk] and
+// *counter zero on entry.
+int trsv_chain_f64(bool lower, bool colmajor, const double* w, int64_t ldw, int n, const double* dinv, double* x,
+                   int64_t ldx, int kc, int* flags, int* counter, unsigned* status, cudaStream_t stream);
 // Inverts the diagonal blocks of the lower and upper triangles of T, T(i,j) = w[i*ldw+j]
 // (w[j*ldw+i] when colmajor), a unit triangle's diagonal taken as 1.
 int invert_diag_blocks_f64(const double* w, int64_t ldw, bool colmajor, int64_t n, double* dinv, bool lower_unit,
@@ -173,6 +179,14 @@ size_t gmres_scratch_bytes(int64_t n, int64_t k, int restart);
 int gmres_ir(const double* a, int64_t n, const double* b, int64_t k, double* x, const Precond& pc, int restart,
              int max_outer, double tol, double* berr_out, int* outer_out, void* scratch, double* r, double* norms,
              double* berr_dev, cudaStream_t s);
+
+// ---------------------------------------------------------------- Cholesky (potrf.cu)
+size_t potrf_f64_scratch_bytes(int64_t n);
+// L (row-major n x n, zeros above the diagonal) of the row-major a's lower triangle; when
+// notpd_host is not NULL, *notpd_host (host memory) gets 1 once the stream reaches that point
+// if a pivot was not > 0.
+int potrf_f64(const double* a, int64_t n, double* l, void* scratch, int* notpd_host, unsigned* status,
+              cudaStream_t stream);
 
 // ---------------------------------------------------------------- helpers (api.cu)
 int64_t round_up(int64_t x, int64_t m);

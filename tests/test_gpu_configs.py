@@ -1,10 +1,14 @@
 """Parity at the benchmarked configurations, against the oracle (rustymath's algorithms
 restated in C), on the same inputs the benchmark builds (bench.make_system, bench.make_batch):
 
-- the single large system, n = 8192 with 16 right-hand sides and kappa = 1e4: the plain
-  float64 LU within n eps (normwise, relative) of the oracle's solution, the mixed method
-  within kappa n eps; both at normwise backward error <= n 2^-53 by the oracle's double-double
-  residual;
+- the single large system, n = 8192 with 16 right-hand sides and kappa = 1e4: both methods
+  within kappa n eps (normwise, relative) of the oracle's solution, at normwise backward error
+  <= n 2^-53 by the oracle's double-double residual, and the plain float64 LU no farther from
+  the oracle than 4 times a third float64 LU (LAPACK getrf + getrs) is. At this kappa two
+  backward-stable float64 solves with different rounding orders differ by about kappa times
+  their backward errors (measured: 9e-12, against n eps = 1.8e-12), so n eps is not a bar any
+  float64 LU other than the oracle's own operation order can meet here; the batched
+  configuration below (kappa < 10) is held to n eps;
 - 20,000 uneven systems (n ~ U{8..256}, A = N(0,1) + n I): a seeded sample of 500 systems,
   the plain method within n eps of the oracle, the mixed one within kappa_inf n eps, and every
   sampled system's backward error <= n 2^-53;
@@ -43,7 +47,10 @@ def test_single_large_system_matches_the_oracle(rb):
     x_mixed, reps = rb.solve_report(a, b, method="mixed")
     x_mixed = x_mixed.cpu().numpy()
     assert reps[0].fell_back == 0 and reps[0].method_used == 1
-    assert _fwd(x_plain, xo) <= n * EPS
+    import scipy.linalg as sl
+    lapack = sl.lu_solve(sl.lu_factor(a_h, check_finite=False), b_h, check_finite=False)
+    assert _fwd(x_plain, xo) <= 1e4 * n * EPS
+    assert _fwd(x_plain, xo) <= 4 * _fwd(lapack, xo)
     assert _fwd(x_mixed, xo) <= 1e4 * n * EPS
     assert O.backward_error(a_h, x_plain, b_h) <= n * 2.0 ** -53
     assert O.backward_error(a_h, x_mixed, b_h) <= n * 2.0 ** -53

@@ -203,3 +203,55 @@ def test_golden_fixtures():
             assert O.lu_determinant(f, p) == case["det"], case["name"]
         if "regular" in case:
             assert O.regular(a, f) == case["regular"], case["name"]
+
+
+def _spd(n, seed):
+    """tests/linalg.rs:391-392: A A^T + n I from the reference's random matrix."""
+    a = ref_random(n, n, seed)
+    return product(a, a.T) + n * np.eye(n)
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 5, 31, 32, 33, 71])
+def test_cholesky_decompositions(n):
+    """tests/linalg.rs:391-399: L is lower triangular, L L^T within 4 eps n of the matrix, and
+    a negative definite matrix has no factor."""
+    spd = _spd(n, n + 1)
+    l = O.cholesky(spd)
+    assert l is not None
+    assert (np.triu(l, 1) == 0).all()
+    assert distance(product(l, l.T), spd, max(norm(spd), 1.0)) < 4 * EPS * max(n, 1)
+    if n > 0:
+        assert O.cholesky(-spd) is None
+
+
+@pytest.mark.parametrize("n", [530, 1030])
+def test_cholesky_blocked(n):
+    """tests/linalg.rs:584-589: (A + A^T)/2 + n I through random vectors."""
+    a = ref_random(n, n, n)
+    x = ref_random(n, 1, 3)
+    spd = (a + a.T) / 2 + n * np.eye(n)
+    l = O.cholesky(spd)
+    assert (np.triu(l, 1) == 0).all()
+    assert distance(product(l, product(l.T, x)), product(spd, x), norm(spd) * norm(x)) < 4 * EPS * n
+
+
+def test_cholesky_scaling_is_exact():
+    """tests/linalg.rs:485-486: a power-of-two scale c (doubled when odd) scales L by sqrt(c)
+    exactly."""
+    n = 40
+    a = ref_random(n, n, 17)
+    spd = product(a, a.T) + n * np.eye(n)
+    tiny = np.finfo(np.float64).tiny / EPS
+    quartic = 2.0 ** (int(np.log2(np.finfo(np.float64).max) / 4.0) + 6)
+    base = O.cholesky(spd)
+    for s in [tiny, 1.0 / tiny, quartic]:
+        c = s if np.sqrt(s) * np.sqrt(s) == s else s + s
+        assert np.array_equal(O.cholesky(spd * c), base * np.sqrt(c))
+
+
+def test_cholesky_vs_numpy():
+    """tests/test_linalg.py:109-110: a a^T + 5 I against numpy.linalg.cholesky."""
+    a = np.random.default_rng(0).standard_normal((5, 5))
+    spd = a @ a.T + 5 * np.eye(5)
+    assert np.allclose(O.cholesky(spd), np.linalg.cholesky(spd))
+    assert O.cholesky(-np.eye(2)) is None
