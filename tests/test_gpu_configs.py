@@ -102,6 +102,6 @@ def test_matmul_2048_matches_the_oracle(rb):
     mag = np.abs(a) @ np.abs(b)
     ta, tb = torch.tensor(a, device="cuda"), torch.tensor(b, device="cuda")
     native = rb.matmul(ta, tb).cpu().numpy()
-    ozaki = rb.matmul_ozaki(ta, tb, slices=8).cpu().numpy()
+    ozaki = rb.linalg.matmul_ozaki(ta, tb, slices=8).cpu().numpy()
     assert (np.abs(native - ref) <= n * EPS * mag).all()
     assert (np.abs(ozaki - ref) <= n * EPS * mag).all()
