@@ -55,10 +55,71 @@ struct Smem {
   alignas(16) double rs[NMAX][KMAX + 1];                  //  padded: a warp's rows on distinct banks)
   alignas(16) double vsm[32][KMAX + 1];                   // a diagonal block's right-hand sides
   int piv[NMAX];                                          // logical position -> row
+  int act[NMAX];                                          // the rows still unchosen after a panel
+  int wcnt[WARPS];
   double red[WARPS][3 * KMAX + 1];
   double anorm, bnorm[KMAX];
   int zero_pivot;
 };
+
+// Rows of the panel multipliers (staged in xs..rs during a factorization) and of U12 (ubt): 144
+// bytes, so that a quarter-warp's 16-byte accesses to consecutive rows fall on distinct banks.
+template <typename T>
+struct Stage {
+  static constexpr int LDU = 144 / (int)sizeof(T);
+};
+static_assert(offsetof(Smem, rs) == offsetof(Smem, xs) + sizeof(Smem::xs), "xs and rs are adjacent");
+static_assert(sizeof(Smem::xs) + sizeof(Smem::rs) >= (size_t)NMAX * 144, "the multipliers fit in xs..rs");
+static_assert(UBT_BYTES >= NMAX * 144, "U12 fits in ubt");
+
+// n items of a row into registers, 16-byte loads when the whole panel is there (rows and panel
+// starts are 16-byte aligned: ld % 4 == 0, panels start at multiples of NB)
+template <typename T, int NB>
+__device__ __forceinline__ void load_row(const T* src, int cnt, T (&v)[NB]) {
+  if (cnt == NB) {
+    constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+    for (int q = 0; q < NB; q += PER) {
+      if constexpr (sizeof(T) == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(src + q);
+        v[q] = t.x, v[q + 1] = t.y, v[q + 2] = t.z, v[q + 3] = t.w;
+      } else {
+        const double2 t = *reinterpret_cast<const double2*>(src + q);
+        v[q] = t.x, v[q + 1] = t.y;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < NB; ++q) v[q] = q < cnt ? src[q] : T(0);
+  }
+}
+
+template <typename T, int NB>
+__device__ __forceinline__ void store_vec(T* dst, const T (&v)[NB]) {
+  constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+  for (int q = 0; q < NB; q += PER) {
+    if constexpr (sizeof(T) == 4)
+      *reinterpret_cast<float4*>(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+    else
+      *reinterpret_cast<double2*>(dst + q) = make_double2(v[q], v[q + 1]);
+  }
+}
+
+template <typename T, int NB>
+__device__ __forceinline__ void load_vec(const T* src, T (&v)[NB]) {
+  constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+  for (int q = 0; q < NB; q += PER) {
+    if constexpr (sizeof(T) == 4) {
+      const float4 t = *reinterpret_cast<const float4*>(src + q);
+      v[q] = t.x, v[q + 1] = t.y, v[q + 2] = t.z, v[q + 3] = t.w;
+    } else {
+      const double2 t = *reinterpret_cast<const double2*>(src + q);
+      v[q] = t.x, v[q + 1] = t.y;
+    }
+  }
+}
 
 template <typename T>
 __device__ __forceinline__ T tabs(T v) {
@@ -103,8 +164,11 @@ template <typename T, int NB>
 __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r = tid;
+  constexpr int LDU = Stage<T>::LDU;
+  static_assert(NB <= LDU, "a staged row holds the panel");
   T(*Lp)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(sm.lp);
-  T(*UbT)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(sm.ubt);
+  T* UbT = reinterpret_cast<T*>(sm.ubt);   // NMAX x LDU: column j of U12 at UbT[j * LDU]
+  T* Lsm = reinterpret_cast<T*>(sm.xs);    // NMAX x LDU: row r's panel multipliers (xs..rs are free here)
   bool active = r < n;
   my_pos = -1;
   for (int J = 0; J < n; J += NB) {
@@ -112,8 +176,10 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
     const bool was_active = active;
     T p[NB];
     T* row = W + (int64_t)r * ld + J;
+    if (active) load_row<T, NB>(row, nbj, p);
+    else
 #pragma unroll
-    for (int i = 0; i < NB; ++i) p[i] = (active && i < nbj) ? row[i] : T(0);
+      for (int i = 0; i < NB; ++i) p[i] = T(0);
 #pragma unroll
     for (int c = 0; c < NB; ++c) {
       if (c < nbj) {
@@ -193,8 +259,20 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
       for (int i = 0; i < NB; ++i)
         if (i < nbj) row[i] = p[i];
     }
-    __syncthreads();
     const int rc0 = J + nbj, rcols = n - rc0;
+    // the rows still unchosen, in increasing order, and their multipliers in shared memory
+    const unsigned ball = __ballot_sync(0xffffffffu, active);
+    if (lane == 0) sm.wcnt[warp] = __popc(ball);
+    if (active && rcols > 0) store_vec<T, NB>(Lsm + r * LDU, p);
+    __syncthreads();
+    int base = 0, nact = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+      const int c = sm.wcnt[w];
+      base += w < warp ? c : 0;
+      nact += c;
+    }
+    if (active) sm.act[base + __popc(ball & ((1u << lane) - 1u))] = r;
     if (rcols > 0) {
       // U12 of the panel's pivot rows: u = Lp^-1 (their later columns), a column per thread
       for (int j = tid; j < rcols; j += THREADS) {
@@ -206,21 +284,61 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
 #pragma unroll
           for (int q = 0; q < c; ++q) u[c] = fma(-Lp[c][q], u[q], u[c]);
 #pragma unroll
-        for (int c = 0; c < NB; ++c) {
+        for (int c = 0; c < NB; ++c)
           if (c < nbj) W[(int64_t)sm.piv[J + c] * ld + rc0 + j] = u[c];
-          UbT[j][c] = u[c];
-        }
+        store_vec<T, NB>(UbT + j * LDU, u);
       }
       __syncthreads();
-      // the rows not chosen yet: later columns -= L(row, panel) U12
-      if (active) {
-        T* rrow = W + (int64_t)r * ld + rc0;
-#pragma unroll 4
-        for (int j = 0; j < rcols; ++j) {
-          T acc = rrow[j];
+      // the rows not chosen yet: later columns -= L(row, panel) U12, a thread per column (reads of
+      // a row's columns coalesced across the warp), the U12 column in registers, the row's
+      // multipliers broadcast from shared memory; when the columns are few, groups of threads
+      // take interleaved rows
+      const int width = (rcols + 31) & ~31;
+      const int groups = THREADS / width;
+      const int g = tid / width, j = tid - g * width;
+      if (g < groups && j < rcols) {
+        T u[NB];
+        load_vec<T, NB>(UbT + j * LDU, u);
+        T* col = W + rc0 + j;
+        int idx = g;
+        for (; idx + 3 * groups < nact; idx += 4 * groups) {
+          const int r0 = sm.act[idx], r1 = sm.act[idx + groups], r2 = sm.act[idx + 2 * groups],
+                    r3 = sm.act[idx + 3 * groups];
+          T x0 = col[(int64_t)r0 * ld], x1 = col[(int64_t)r1 * ld], x2 = col[(int64_t)r2 * ld],
+            x3 = col[(int64_t)r3 * ld];
+          constexpr int PER = 16 / (int)sizeof(T);
 #pragma unroll
-          for (int c = 0; c < NB; ++c) acc = fma(-p[c], UbT[j][c], acc);
-          rrow[j] = acc;
+          for (int c = 0; c < NB; c += PER) {
+            T a0[PER], a1[PER], a2[PER], a3[PER];
+            load_vec<T, PER>(Lsm + r0 * LDU + c, a0);
+            load_vec<T, PER>(Lsm + r1 * LDU + c, a1);
+            load_vec<T, PER>(Lsm + r2 * LDU + c, a2);
+            load_vec<T, PER>(Lsm + r3 * LDU + c, a3);
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+              x0 = fma(-a0[q], u[c + q], x0);
+              x1 = fma(-a1[q], u[c + q], x1);
+              x2 = fma(-a2[q], u[c + q], x2);
+              x3 = fma(-a3[q], u[c + q], x3);
+            }
+          }
+          col[(int64_t)r0 * ld] = x0;
+          col[(int64_t)r1 * ld] = x1;
+          col[(int64_t)r2 * ld] = x2;
+          col[(int64_t)r3 * ld] = x3;
+        }
+        for (; idx < nact; idx += groups) {
+          const int r0 = sm.act[idx];
+          T x0 = col[(int64_t)r0 * ld];
+          constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+          for (int c = 0; c < NB; c += PER) {
+            T a0[PER];
+            load_vec<T, PER>(Lsm + r0 * LDU + c, a0);
+#pragma unroll
+            for (int q = 0; q < PER; ++q) x0 = fma(-a0[q], u[c + q], x0);
+          }
+          col[(int64_t)r0 * ld] = x0;
         }
       }
     }
@@ -261,13 +379,14 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
     __syncthreads();
     if (r < n) {
       if (my_pos >= J + nbj) {
+        T lv[NB];
+        load_row<T, NB>(row + J, nbj, lv);
 #pragma unroll
         for (int q = 0; q < NB; ++q)
           if (q < nbj) {
-            const T l = row[J + q];
 #pragma unroll
             for (int c = 0; c < KK; ++c)
-              if (c < k) v[c] = fma(-l, (T)sm.vsm[q][c], v[c]);
+              if (c < k) v[c] = fma(-lv[q], (T)sm.vsm[q][c], v[c]);
           }
       } else if (my_pos >= J) {
 #pragma unroll
@@ -304,13 +423,14 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
     __syncthreads();
     if (r < n) {
       if (my_pos >= 0 && my_pos < J) {
+        T uv[NB];
+        load_row<T, NB>(row + J, nbj, uv);
 #pragma unroll
         for (int q = 0; q < NB; ++q)
           if (q < nbj) {
-            const T u = row[J + q];
 #pragma unroll
             for (int c = 0; c < KK; ++c)
-              if (c < k) v[c] = fma(-u, (T)sm.vsm[q][c], v[c]);
+              if (c < k) v[c] = fma(-uv[q], (T)sm.vsm[q][c], v[c]);
           }
       } else if (my_pos >= J && my_pos < J + nbj) {
 #pragma unroll
@@ -340,13 +460,19 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
     double acc[KK], asum = 0.0;
 #pragma unroll
     for (int c = 0; c < KK; ++c) acc[c] = 0.0;
-#pragma unroll 4
-    for (int j = lane; j < n; j += 32) {
-      const double av = __ldg(ar + j);
-      asum += fabs(av);
+    // the lane's items of the row, all in flight before the first is used
+    double av[NMAX / 32];
 #pragma unroll
-      for (int c = 0; c < KK; ++c)
-        if (c < k) acc[c] = fma(av, sm.xs[j][c], acc[c]);
+    for (int q = 0; q < NMAX / 32; ++q) av[q] = lane + 32 * q < n ? __ldg(ar + lane + 32 * q) : 0.0;
+#pragma unroll
+    for (int q = 0; q < NMAX / 32; ++q) {
+      const int j = lane + 32 * q;
+      if (j < n) {
+        asum += fabs(av[q]);
+#pragma unroll
+        for (int c = 0; c < KK; ++c)
+          if (c < k) acc[c] = fma(av[q], sm.xs[j][c], acc[c]);
+      }
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
