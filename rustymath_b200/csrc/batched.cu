@@ -56,6 +56,7 @@ struct Smem {
   alignas(16) double vsm[32][KMAX + 1];                   // a diagonal block's right-hand sides
   int piv[NMAX];                                          // logical position -> row
   int act[NMAX];                                          // the rows still unchosen after a panel
+  double colsum[NMAX];                                    // column sums of |a| (dominance test)
   int wcnt[WARPS];
   double red[WARPS][3 * KMAX + 1];
   double anorm, bnorm[KMAX];
@@ -156,12 +157,139 @@ __device__ void load_w(const double* __restrict__ a, int n, T* W, int ld) {
     for (int j = lane; j < n; j += 32) W[(int64_t)r * ld + j] = (T)__ldcs(a + (int64_t)r * n + j);
 }
 
+// Relative margin of the column diagonal dominance that lets a factorization skip the pivot
+// search: |a_jj| - sum_{i != j} |a_ij| > kDominance * sum_i |a_ij| for every column j.
+constexpr double kDominance = 1e-10;
+
+// load_w, and whether a is strictly column diagonally dominant with the margin kDominance
+// (the same answer in every thread). On such a matrix partial pivoting chooses the diagonal at
+// every step: the Schur complements of a column diagonally dominant matrix keep that dominance
+// with at least the same excess, so in column c the diagonal item is larger than the sum, and so
+// than the largest, of the others below it. The margin covers the float64 rounding of the
+// updates (growth at most 2, n <= 256: far below 1e-10 of a column's sum); NaN or a zero column
+// fail the test.
+template <typename T>
+__device__ bool load_w_dominant(const double* __restrict__ a, int n, T* W, int ld, Smem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j = threadIdx.x; j < NMAX; j += THREADS) sm.colsum[j] = 0.0;
+  __syncthreads();
+  double cs[NMAX / 32];
+#pragma unroll
+  for (int q = 0; q < NMAX / 32; ++q) cs[q] = 0.0;
+  for (int r = warp; r < n; r += WARPS) {
+#pragma unroll
+    for (int q = 0; q < NMAX / 32; ++q) {
+      const int j = lane + 32 * q;
+      if (j < n) {
+        const double v = __ldcs(a + (int64_t)r * n + j);
+        W[(int64_t)r * ld + j] = (T)v;
+        cs[q] += fabs(v);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NMAX / 32; ++q)
+    if (lane + 32 * q < n) atomicAdd(&sm.colsum[lane + 32 * q], cs[q]);
+  __syncthreads();
+  bool ok = true;
+  const int j = threadIdx.x;
+  if (j < n) {
+    const double d = fabs(a[(int64_t)j * n + j]), sum = sm.colsum[j];
+    ok = d - (sum - d) > kDominance * sum;  // false for NaN
+  }
+  return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// After a panel (columns J..J+nbj) is factored: the pivot rows' later columns become U12 =
+// L11^-1 A12 (a column per thread; U12 to shared memory) and the nact rows still unchosen,
+// sm.act[0..nact) with their multipliers in Lsm, take A22 -= L21 U12. A thread per column does
+// the update (reads of a row's columns are coalesced across the warp), the U12 column in
+// registers and the row's multipliers broadcast from shared memory; when the columns are few,
+// groups of threads take interleaved rows. Ends before the closing barrier.
+template <typename T, int NB>
+__device__ __forceinline__ void panel_tail(T* W, int ld, int n, Smem& sm, int J, int nbj, int nact) {
+  const int tid = threadIdx.x;
+  constexpr int LDU = Stage<T>::LDU;
+  T(*Lp)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(sm.lp);
+  T* UbT = reinterpret_cast<T*>(sm.ubt);
+  const T* Lsm = reinterpret_cast<const T*>(sm.xs);
+  const int rc0 = J + nbj, rcols = n - rc0;
+  if (rcols <= 0) return;
+    // U12 of the panel's pivot rows: u = Lp^-1 (their later columns), a column per thread
+    for (int j = tid; j < rcols; j += THREADS) {
+      T u[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) u[c] = c < nbj ? W[(int64_t)sm.piv[J + c] * ld + rc0 + j] : T(0);
+#pragma unroll
+      for (int c = 1; c < NB; ++c)
+#pragma unroll
+        for (int q = 0; q < c; ++q) u[c] = fma(-Lp[c][q], u[q], u[c]);
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < nbj) W[(int64_t)sm.piv[J + c] * ld + rc0 + j] = u[c];
+      store_vec<T, NB>(UbT + j * LDU, u);
+    }
+    __syncthreads();
+    // the rows not chosen yet: later columns -= L(row, panel) U12, a thread per column (reads of
+    // a row's columns coalesced across the warp), the U12 column in registers, the row's
+    // multipliers broadcast from shared memory; when the columns are few, groups of threads
+    // take interleaved rows
+    const int width = (rcols + 31) & ~31;
+    const int groups = THREADS / width;
+    const int g = tid / width, j = tid - g * width;
+    if (g < groups && j < rcols) {
+      T u[NB];
+      load_vec<T, NB>(UbT + j * LDU, u);
+      T* col = W + rc0 + j;
+      int idx = g;
+      for (; idx + 3 * groups < nact; idx += 4 * groups) {
+        const int r0 = sm.act[idx], r1 = sm.act[idx + groups], r2 = sm.act[idx + 2 * groups],
+                  r3 = sm.act[idx + 3 * groups];
+        T x0 = col[(int64_t)r0 * ld], x1 = col[(int64_t)r1 * ld], x2 = col[(int64_t)r2 * ld],
+          x3 = col[(int64_t)r3 * ld];
+        constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+        for (int c = 0; c < NB; c += PER) {
+          T a0[PER], a1[PER], a2[PER], a3[PER];
+          load_vec<T, PER>(Lsm + r0 * LDU + c, a0);
+          load_vec<T, PER>(Lsm + r1 * LDU + c, a1);
+          load_vec<T, PER>(Lsm + r2 * LDU + c, a2);
+          load_vec<T, PER>(Lsm + r3 * LDU + c, a3);
+#pragma unroll
+          for (int q = 0; q < PER; ++q) {
+            x0 = fma(-a0[q], u[c + q], x0);
+            x1 = fma(-a1[q], u[c + q], x1);
+            x2 = fma(-a2[q], u[c + q], x2);
+            x3 = fma(-a3[q], u[c + q], x3);
+          }
+        }
+        col[(int64_t)r0 * ld] = x0;
+        col[(int64_t)r1 * ld] = x1;
+        col[(int64_t)r2 * ld] = x2;
+        col[(int64_t)r3 * ld] = x3;
+      }
+      for (; idx < nact; idx += groups) {
+        const int r0 = sm.act[idx];
+        T x0 = col[(int64_t)r0 * ld];
+        constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+        for (int c = 0; c < NB; c += PER) {
+          T a0[PER];
+          load_vec<T, PER>(Lsm + r0 * LDU + c, a0);
+#pragma unroll
+          for (int q = 0; q < PER; ++q) x0 = fma(-a0[q], u[c + q], x0);
+        }
+        col[(int64_t)r0 * ld] = x0;
+      }
+    }
+}
+
 // Implicitly pivoted LU of the n x n W (row-major, ld): thread r owns row r; my_pos (in/out)
 // is the logical position of row r, -1 before it is chosen; sm.piv[c] is the row chosen for
 // column c. Returns with every thread's my_pos set. A zero pivot sets sm.zero_pivot and
 // leaves its column unreduced.
 template <typename T, int NB>
-__device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
+__device__ void bfactor_pivoted(T* W, int ld, int n, Smem& sm, int& my_pos) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r = tid;
   constexpr int LDU = Stage<T>::LDU;
@@ -273,77 +401,98 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos) {
       nact += c;
     }
     if (active) sm.act[base + __popc(ball & ((1u << lane) - 1u))] = r;
-    if (rcols > 0) {
-      // U12 of the panel's pivot rows: u = Lp^-1 (their later columns), a column per thread
-      for (int j = tid; j < rcols; j += THREADS) {
-        T u[NB];
+    panel_tail<T, NB>(W, ld, n, sm, J, nbj, nact);
+    __syncthreads();
+  }
+}
+
+// The factorization of a matrix that load_w_dominant found column diagonally dominant: the
+// pivot of column c is row c, so there is no pivot search and no barrier per column. Per
+// panel, warp 0 factors the diagonal block with its rows in registers (lane i holds row J + i,
+// the pivot row's items passed by shuffles), then every row below solves its own multipliers
+// against U11 from shared memory, then panel_tail. Every item is computed by the same
+// operations in the same order as bfactor_pivoted would with those pivots, so the results
+// are the same bits.
+template <typename T, int NB>
+__device__ void bfactor_dominant(T* W, int ld, int n, Smem& sm, int& my_pos) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r = tid;
+  constexpr int LDU = Stage<T>::LDU;
+  T(*Lp)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(sm.lp);
+  T* Lsm = reinterpret_cast<T*>(sm.xs);
+  my_pos = r < n ? r : -1;
+  for (int i = tid; i < n; i += THREADS) sm.piv[i] = i;
+  for (int J = 0; J < n; J += NB) {
+    const int nbj = min(NB, n - J);
+    const int rc0 = J + nbj, rcols = n - rc0;
+    if (warp == 0) {
+      const bool mine = lane < nbj;
+      T p[NB];
+      if (mine) load_row<T, NB>(W + (int64_t)(J + lane) * ld + J, nbj, p);
+      else
 #pragma unroll
-        for (int c = 0; c < NB; ++c) u[c] = c < nbj ? W[(int64_t)sm.piv[J + c] * ld + rc0 + j] : T(0);
+        for (int i = 0; i < NB; ++i) p[i] = T(0);
 #pragma unroll
-        for (int c = 1; c < NB; ++c)
+      for (int c = 0; c < NB; ++c) {
+        if (c < nbj) {
+          T prow[NB];
 #pragma unroll
-          for (int q = 0; q < c; ++q) u[c] = fma(-Lp[c][q], u[q], u[c]);
+          for (int i = c; i < NB; ++i) prow[i] = __shfl_sync(0xffffffffu, p[i], c);
+          const T piv = prow[c];
+          if (lane > c && mine && piv != T(0)) {
+            const T l = bdivide(p[c], piv);
+            p[c] = l;
 #pragma unroll
-        for (int c = 0; c < NB; ++c)
-          if (c < nbj) W[(int64_t)sm.piv[J + c] * ld + rc0 + j] = u[c];
-        store_vec<T, NB>(UbT + j * LDU, u);
-      }
-      __syncthreads();
-      // the rows not chosen yet: later columns -= L(row, panel) U12, a thread per column (reads of
-      // a row's columns coalesced across the warp), the U12 column in registers, the row's
-      // multipliers broadcast from shared memory; when the columns are few, groups of threads
-      // take interleaved rows
-      const int width = (rcols + 31) & ~31;
-      const int groups = THREADS / width;
-      const int g = tid / width, j = tid - g * width;
-      if (g < groups && j < rcols) {
-        T u[NB];
-        load_vec<T, NB>(UbT + j * LDU, u);
-        T* col = W + rc0 + j;
-        int idx = g;
-        for (; idx + 3 * groups < nact; idx += 4 * groups) {
-          const int r0 = sm.act[idx], r1 = sm.act[idx + groups], r2 = sm.act[idx + 2 * groups],
-                    r3 = sm.act[idx + 3 * groups];
-          T x0 = col[(int64_t)r0 * ld], x1 = col[(int64_t)r1 * ld], x2 = col[(int64_t)r2 * ld],
-            x3 = col[(int64_t)r3 * ld];
-          constexpr int PER = 16 / (int)sizeof(T);
-#pragma unroll
-          for (int c = 0; c < NB; c += PER) {
-            T a0[PER], a1[PER], a2[PER], a3[PER];
-            load_vec<T, PER>(Lsm + r0 * LDU + c, a0);
-            load_vec<T, PER>(Lsm + r1 * LDU + c, a1);
-            load_vec<T, PER>(Lsm + r2 * LDU + c, a2);
-            load_vec<T, PER>(Lsm + r3 * LDU + c, a3);
-#pragma unroll
-            for (int q = 0; q < PER; ++q) {
-              x0 = fma(-a0[q], u[c + q], x0);
-              x1 = fma(-a1[q], u[c + q], x1);
-              x2 = fma(-a2[q], u[c + q], x2);
-              x3 = fma(-a3[q], u[c + q], x3);
-            }
+            for (int i = c + 1; i < NB; ++i) p[i] = fma(-l, prow[i], p[i]);
           }
-          col[(int64_t)r0 * ld] = x0;
-          col[(int64_t)r1 * ld] = x1;
-          col[(int64_t)r2 * ld] = x2;
-          col[(int64_t)r3 * ld] = x3;
+          if (piv == T(0) && lane == 0) sm.zero_pivot = 1;
         }
-        for (; idx < nact; idx += groups) {
-          const int r0 = sm.act[idx];
-          T x0 = col[(int64_t)r0 * ld];
-          constexpr int PER = 16 / (int)sizeof(T);
+      }
+      if (mine) {
+        T* row = W + (int64_t)(J + lane) * ld + J;
 #pragma unroll
-          for (int c = 0; c < NB; c += PER) {
-            T a0[PER];
-            load_vec<T, PER>(Lsm + r0 * LDU + c, a0);
-#pragma unroll
-            for (int q = 0; q < PER; ++q) x0 = fma(-a0[q], u[c + q], x0);
-          }
-          col[(int64_t)r0 * ld] = x0;
+        for (int i = 0; i < NB; ++i) {
+          if (i < nbj) row[i] = p[i];
+          Lp[lane][i] = p[i];
         }
       }
     }
     __syncthreads();
+    // the rows below the block: their multipliers, against U11 in Lp
+    if (r >= rc0 && r < n) {
+      T p[NB];
+      T* row = W + (int64_t)r * ld + J;
+      load_row<T, NB>(row, nbj, p);
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        if (c < nbj) {
+          const T piv = Lp[c][c];
+          if (piv != T(0)) {
+            const T l = bdivide(p[c], piv);
+            p[c] = l;
+#pragma unroll
+            for (int i = c + 1; i < NB; ++i) p[i] = fma(-l, Lp[c][i], p[i]);
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < NB; ++i)
+        if (i < nbj) row[i] = p[i];
+      if (rcols > 0) store_vec<T, NB>(Lsm + r * LDU, p);
+    }
+    for (int i = tid; i < rcols; i += THREADS) sm.act[i] = rc0 + i;
+    panel_tail<T, NB>(W, ld, n, sm, J, nbj, rcols);
+    __syncthreads();
   }
+}
+
+// LU of the n x n W (row-major, ld) with partial pivoting: thread r owns row r; on return
+// my_pos is the logical position of row r and sm.piv[c] the row chosen for column c. A zero
+// pivot sets sm.zero_pivot and leaves its column unreduced.
+template <typename T, int NB>
+__device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos, bool dominant) {
+  if (dominant) bfactor_dominant<T, NB>(W, ld, n, sm, my_pos);
+  else bfactor_pivoted<T, NB>(W, ld, n, sm, my_pos);
 }
 
 // Solves L U x = P v: thread r holds v (its row's k right-hand sides) on entry and x[my_pos]
@@ -578,10 +727,10 @@ struct Batch {
 template <typename T, int NB, int KK>
 __device__ bool factor_and_solve(Batch& bt, Smem& sm, int n, int k, int ld, T* W, const double* a, const double* b,
                                  int& my_pos) {
-  load_w<T>(a, n, W, ld);
+  const bool dominant = load_w_dominant<T>(a, n, W, ld, sm);
   if (threadIdx.x == 0) sm.zero_pivot = 0;
   __syncthreads();
-  bfactor<T, NB>(W, ld, n, sm, my_pos);
+  bfactor<T, NB>(W, ld, n, sm, my_pos, dominant);
   T v[KK];
 #pragma unroll
   for (int c = 0; c < KK; ++c) v[c] = (threadIdx.x < n && c < k) ? (T)b[(int64_t)threadIdx.x * k + c] : T(0);
@@ -920,10 +1069,9 @@ __global__ void __launch_bounds__(THREADS, 2) batch_adjoint_kernel(Adjoint aj) {
       // float64 factors (the forward's, or made here when float32 refinement stalls)
       double* W = reinterpret_cast<double*>(w);
       if (bt.ftype[s] == 0) {
-        load_w<double>(a, n, W, ld);
-        __syncthreads();
+        const bool dominant = load_w_dominant<double>(a, n, W, ld, sm);
         int my_pos;
-        bfactor<double, 16>(W, ld, n, sm, my_pos);
+        bfactor<double, 16>(W, ld, n, sm, my_pos, dominant);
         for (int i = threadIdx.x; i < n; i += THREADS) bt.piv[bt.p_off[s] + i] = sm.piv[i];
         if (threadIdx.x == 0) bt.ftype[s] = 1;
         __syncthreads();
@@ -968,14 +1116,14 @@ __global__ void __launch_bounds__(THREADS) batch_factor_kernel(const double* __r
   const int ld = (n + 3) & ~3;
   double* W = reinterpret_cast<double*>(wbuf + m * w_stride);
   const double* am = a + m * n * n;
-  load_w<double>(am, n, W, ld);
+  const bool dominant = load_w_dominant<double>(am, n, W, ld, sm);
   if (threadIdx.x == 0) {
     sm.zero_pivot = 0;
     irregular = 0;
   }
   __syncthreads();
   int my_pos = -1;
-  bfactor<double, 16>(W, ld, n, sm, my_pos);
+  bfactor<double, 16>(W, ld, n, sm, my_pos, dominant);
   double* fm = factors + m * n * n;
   for (int e = threadIdx.x; e < n * n; e += THREADS) {
     const int j = e / n, i = e - j * n;

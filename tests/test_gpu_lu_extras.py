@@ -153,3 +153,26 @@ def test_dtype_ladder(rb):
     assert rb.lu(ai).p.dtype == np.int64
     with pytest.raises(TypeError):
         rb.solve(ai.astype(np.complex128), np.array([1, 2]))
+
+
+@pytest.mark.parametrize("n", [8, 33, 160, 256])
+def test_dominant_stacks_take_the_oracles_pivots(rb, n):
+    """Column diagonally dominant matrices (N(0,1) + 2n I) factor without a pivot search on the
+    GPU; partial pivoting chooses their diagonal at every step, so the row positions are the
+    identity, as the oracle's, and the factors agree with the oracle's; a stack mixing them with
+    general matrices takes both routes in one launch."""
+    rng = np.random.default_rng(n + 100)
+    stack = rng.standard_normal((10, n, n))
+    stack[::2] += 2 * n * np.eye(n)
+    f = rb.lu(stack)
+    for i in range(10):
+        fo, po = O.lu_factor(stack[i])
+        assert np.array_equal(f.p[i], po), i
+        if i % 2 == 0:
+            assert np.array_equal(po, np.arange(n))
+        assert np.abs(f.factors[i] - fo).max() <= 1e3 * n * EPS * np.abs(fo).max()
+    b = rng.standard_normal((10, n, 3))
+    for method in ("plain", "mixed"):
+        x = rb.solve(stack, b, method=method)
+        for i in range(10):
+            assert O.backward_error(stack[i], x[i], b[i]) <= n * 2.0 ** -53
