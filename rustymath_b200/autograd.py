@@ -14,6 +14,27 @@ from .batched import BatchPlan
 
 __all__ = ["solve", "BatchedSolve"]
 
+# Plans (scratch, sorted order, captured graph) by (device, batch, n, k, method): a training
+# loop solving systems of one shape reuses its plan instead of building one per forward. The
+# forward's factors live in the plan until its backward has run, so a plan is lent to one
+# forward at a time; a second forward of the same shape before the first's backward gets a
+# plan of its own.
+_PLANS = {}
+
+
+def _plan(device, batch, n, k, method):
+    key = (str(device), batch, n, k, method)
+    free = _PLANS.setdefault(key, [])
+    return free.pop() if free else BatchPlan([n] * batch, [k] * batch, method=method), key
+
+
+def _release(key, plan):
+    free = _PLANS.setdefault(key, [])
+    if len(free) < 4:
+        free.append(plan)
+    else:
+        plan.close()
+
 
 class BatchedSolve(torch.autograd.Function):
     """x = A^-1 b for a (batch, n, n) float64 CUDA stack and (batch, n, k) right-hand sides."""
@@ -22,14 +43,17 @@ class BatchedSolve(torch.autograd.Function):
     def forward(ctx, a, b, method):
         batch, n, _ = a.shape
         k = b.shape[-1]
-        plan = BatchPlan([n] * batch, [k] * batch, method=method)
+        plan, key = _plan(a.device, batch, n, k, method)
         af = a.detach().contiguous().view(-1)
         bf = b.detach().contiguous().view(-1)
         x = torch.empty(batch * n * k, dtype=torch.float64, device=a.device)
         if batch:
             plan.execute(af, bf, x)
-        ctx.plan = plan
+        ctx.plan, ctx.key = plan, key
         ctx.shapes = (batch, n, k)
+        if not (ctx.needs_input_grad[0] or ctx.needs_input_grad[1]):
+            _release(key, plan)  # no backward will read the factors
+            ctx.plan = None
         ctx.save_for_backward(af, x)
         return x.view(batch, n, k)
 
@@ -42,6 +66,8 @@ class BatchedSolve(torch.autograd.Function):
         ga = torch.empty(batch * n * n, dtype=torch.float64, device=x.device) if ctx.needs_input_grad[0] else None
         if batch:
             plan.adjoint(af, x, gx.detach().to(torch.float64).contiguous().view(-1), gb, ga)
+        _release(ctx.key, plan)
+        ctx.plan = None
         return (None if ga is None else ga.view(batch, n, n)), gb.view(batch, n, k), None
 
 

@@ -57,6 +57,7 @@ struct Smem {
   int piv[NMAX];                                          // logical position -> row
   int act[NMAX];                                          // the rows still unchosen after a panel
   double colsum[NMAX];                                    // column sums of |a| (dominance test)
+  double amax_a;                                          // max |a_ij|, NaN ignored
   int wcnt[WARPS];
   double red[WARPS][3 * KMAX + 1];
   double anorm, bnorm[KMAX];
@@ -173,24 +174,47 @@ __device__ bool load_w_dominant(const double* __restrict__ a, int n, T* W, int l
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int j = threadIdx.x; j < NMAX; j += THREADS) sm.colsum[j] = 0.0;
   __syncthreads();
-  double cs[NMAX / 32];
+  double cs[NMAX / 32], amax = 0.0;
 #pragma unroll
   for (int q = 0; q < NMAX / 32; ++q) cs[q] = 0.0;
-  for (int r = warp; r < n; r += WARPS) {
+  // two rows per warp at a time: all sixteen of a lane's loads in flight before the first store
+  for (int r = warp; r < n; r += 2 * WARPS) {
+    const int r1 = r + WARPS;
+    double v0[NMAX / 32], v1[NMAX / 32];
+#pragma unroll
+    for (int q = 0; q < NMAX / 32; ++q) {
+      const int j = lane + 32 * q;
+      v0[q] = j < n ? __ldcs(a + (int64_t)r * n + j) : 0.0;
+      v1[q] = (j < n && r1 < n) ? __ldcs(a + (int64_t)r1 * n + j) : 0.0;
+    }
 #pragma unroll
     for (int q = 0; q < NMAX / 32; ++q) {
       const int j = lane + 32 * q;
       if (j < n) {
-        const double v = __ldcs(a + (int64_t)r * n + j);
-        W[(int64_t)r * ld + j] = (T)v;
-        cs[q] += fabs(v);
+        W[(int64_t)r * ld + j] = (T)v0[q];
+        cs[q] += fabs(v0[q]);
+        amax = fmax(amax, fabs(v0[q]));
+        if (r1 < n) {
+          W[(int64_t)r1 * ld + j] = (T)v1[q];
+          cs[q] += fabs(v1[q]);
+          amax = fmax(amax, fabs(v1[q]));
+        }
       }
     }
   }
 #pragma unroll
   for (int q = 0; q < NMAX / 32; ++q)
     if (lane + 32 * q < n) atomicAdd(&sm.colsum[lane + 32 * q], cs[q]);
+  // max |a| ignoring NaN (rustymath's greatest, factor.rs:488), for the regular test
+#pragma unroll
+  for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+  if (lane == 0) sm.red[warp][0] = amax;
   __syncthreads();
+  if (threadIdx.x == 0) {
+    double big = 0.0;
+    for (int w = 0; w < WARPS; ++w) big = fmax(big, sm.red[w][0]);
+    sm.amax_a = big;
+  }
   bool ok = true;
   const int j = threadIdx.x;
   if (j < n) {
@@ -242,11 +266,25 @@ __device__ __forceinline__ void panel_tail(T* W, int ld, int n, Smem& sm, int J,
       load_vec<T, NB>(UbT + j * LDU, u);
       T* col = W + rc0 + j;
       int idx = g;
+      // four rows at a time; the next four rows' items are loaded while these four are updated
+      T n0 = T(0), n1 = T(0), n2 = T(0), n3 = T(0);
+      if (idx + 3 * groups < nact) {
+        n0 = col[(int64_t)sm.act[idx] * ld];
+        n1 = col[(int64_t)sm.act[idx + groups] * ld];
+        n2 = col[(int64_t)sm.act[idx + 2 * groups] * ld];
+        n3 = col[(int64_t)sm.act[idx + 3 * groups] * ld];
+      }
       for (; idx + 3 * groups < nact; idx += 4 * groups) {
         const int r0 = sm.act[idx], r1 = sm.act[idx + groups], r2 = sm.act[idx + 2 * groups],
                   r3 = sm.act[idx + 3 * groups];
-        T x0 = col[(int64_t)r0 * ld], x1 = col[(int64_t)r1 * ld], x2 = col[(int64_t)r2 * ld],
-          x3 = col[(int64_t)r3 * ld];
+        T x0 = n0, x1 = n1, x2 = n2, x3 = n3;
+        const int nxt = idx + 4 * groups;
+        if (nxt + 3 * groups < nact) {
+          n0 = col[(int64_t)sm.act[nxt] * ld];
+          n1 = col[(int64_t)sm.act[nxt + groups] * ld];
+          n2 = col[(int64_t)sm.act[nxt + 2 * groups] * ld];
+          n3 = col[(int64_t)sm.act[nxt + 3 * groups] * ld];
+        }
         constexpr int PER = 16 / (int)sizeof(T);
 #pragma unroll
         for (int c = 0; c < NB; c += PER) {
@@ -426,18 +464,21 @@ __device__ void bfactor_dominant(T* W, int ld, int n, Smem& sm, int& my_pos) {
     const int nbj = min(NB, n - J);
     const int rc0 = J + nbj, rcols = n - rc0;
     if (warp == 0) {
+      // lane i holds row J + i; at step c every lane reads the pivot row (final since step c - 1)
+      // from Lp with 16-byte broadcast loads, and the next pivot row's lane stores its row there
       const bool mine = lane < nbj;
       T p[NB];
       if (mine) load_row<T, NB>(W + (int64_t)(J + lane) * ld + J, nbj, p);
       else
 #pragma unroll
         for (int i = 0; i < NB; ++i) p[i] = T(0);
+      if (lane == 0) store_vec<T, NB>(&Lp[0][0], p);
+      __syncwarp();
 #pragma unroll
       for (int c = 0; c < NB; ++c) {
         if (c < nbj) {
           T prow[NB];
-#pragma unroll
-          for (int i = c; i < NB; ++i) prow[i] = __shfl_sync(0xffffffffu, p[i], c);
+          load_vec<T, NB>(&Lp[c][0], prow);
           const T piv = prow[c];
           if (lane > c && mine && piv != T(0)) {
             const T l = bdivide(p[c], piv);
@@ -446,15 +487,15 @@ __device__ void bfactor_dominant(T* W, int ld, int n, Smem& sm, int& my_pos) {
             for (int i = c + 1; i < NB; ++i) p[i] = fma(-l, prow[i], p[i]);
           }
           if (piv == T(0) && lane == 0) sm.zero_pivot = 1;
+          if (lane == c + 1 && c + 1 < NB) store_vec<T, NB>(&Lp[lane][0], p);
+          __syncwarp();
         }
       }
       if (mine) {
         T* row = W + (int64_t)(J + lane) * ld + J;
 #pragma unroll
-        for (int i = 0; i < NB; ++i) {
+        for (int i = 0; i < NB; ++i)
           if (i < nbj) row[i] = p[i];
-          Lp[lane][i] = p[i];
-        }
       }
     }
     __syncthreads();
@@ -495,6 +536,15 @@ __device__ void bfactor(T* W, int ld, int n, Smem& sm, int& my_pos, bool dominan
   else bfactor_pivoted<T, NB>(W, ld, n, sm, my_pos);
 }
 
+// Copies cnt items of a row segment (16-byte aligned, the row padded to a multiple of 16 bytes
+// past cnt) to shared memory with 16-byte asynchronous copies, in one commit group of the thread.
+template <typename T>
+__device__ __forceinline__ void copy_segment(T* dst, const T* src, int cnt) {
+  constexpr int PER = 16 / (int)sizeof(T);
+  for (int q = 0; q < cnt; q += PER) cp_async16(dst + q, src + q);
+  cp_async_commit();
+}
+
 // Solves L U x = P v: thread r holds v (its row's k right-hand sides) on entry and x[my_pos]
 // on return. W holds the implicitly pivoted factors of bfactor<T, NB>.
 template <typename T, int NB, int KK>
@@ -502,89 +552,89 @@ __device__ void bsolve(const T* W, int ld, int n, int k, Smem& sm, int my_pos, T
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r = tid;
   const T* row = W + (int64_t)r * ld;
-  // forward: blocks of NB logical columns
+  // forward: blocks of NB logical columns. A block's loads (the thread's row segment, and for the
+  // solving warps their row of the diagonal block) are issued first, so that their latency
+  // overlaps the barrier and the shuffle chain instead of following them.
   for (int J = 0; J < n; J += NB) {
     const int nbj = min(NB, n - J);
+    const bool upd = r < n && my_pos >= J + nbj;
+    T* seg = reinterpret_cast<T*>(sm.ubt + r * 144);  // this row's segment, copied asynchronously
+    if (upd) copy_segment<T>(seg, row + J, nbj);
+    T lv[NB];
     if (my_pos >= J && my_pos < J + nbj)
 #pragma unroll
       for (int c = 0; c < KK; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
     __syncthreads();
     if (warp < k) {  // a warp per right-hand side: column c = warp, lane = row of the block
       const int c = warp;
-      T lrow[NB];
-      const T* prow = W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J;
+      load_row<T, NB>(W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J, nbj, lv);
       T y = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
-#pragma unroll
-      for (int q = 0; q < NB; ++q) lrow[q] = (lane < nbj && q < lane) ? prow[q] : T(0);
 #pragma unroll
       for (int q = 0; q < NB; ++q) {
         if (q < nbj) {
           const T yq = __shfl_sync(0xffffffffu, y, q);
-          if (lane > q) y = fma(-lrow[q], yq, y);
+          if (lane > q && lane < nbj) y = fma(-lv[q], yq, y);
         }
       }
       if (lane < nbj) sm.vsm[lane][c] = (double)y;
     }
     __syncthreads();
-    if (r < n) {
-      if (my_pos >= J + nbj) {
-        T lv[NB];
-        load_row<T, NB>(row + J, nbj, lv);
+    if (upd) {
+      cp_async_wait<0>();
+      load_vec<T, NB>(seg, lv);
 #pragma unroll
-        for (int q = 0; q < NB; ++q)
-          if (q < nbj) {
+      for (int q = 0; q < NB; ++q)
+        if (q < nbj) {
 #pragma unroll
-            for (int c = 0; c < KK; ++c)
-              if (c < k) v[c] = fma(-lv[q], (T)sm.vsm[q][c], v[c]);
-          }
-      } else if (my_pos >= J) {
+          for (int c = 0; c < KK; ++c)
+            if (c < k) v[c] = fma(-lv[q], (T)sm.vsm[q][c], v[c]);
+        }
+    } else if (r < n && my_pos >= J && my_pos < J + nbj) {
 #pragma unroll
-        for (int c = 0; c < KK; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
-      }
+      for (int c = 0; c < KK; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
     }
     __syncthreads();
   }
-  // backward
+  // backward, with the same early loads
   const int last = (n - 1) / NB * NB;
   for (int J = last; J >= 0; J -= NB) {
     const int nbj = min(NB, n - J);
+    const bool upd = r < n && my_pos >= 0 && my_pos < J;
+    T* seg = reinterpret_cast<T*>(sm.ubt + r * 144);
+    if (upd) copy_segment<T>(seg, row + J, nbj);
+    T uv[NB];
     if (my_pos >= J && my_pos < J + nbj)
 #pragma unroll
       for (int c = 0; c < KK; ++c) sm.vsm[my_pos - J][c] = (double)v[c];
     __syncthreads();
     if (warp < k) {  // a warp per right-hand side
       const int c = warp;
-      T urow[NB];
-      const T* prow = W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J;
+      load_row<T, NB>(W + (int64_t)(lane < nbj ? sm.piv[J + lane] : 0) * ld + J, nbj, uv);
       T y = lane < nbj ? (T)sm.vsm[lane][c] : T(0);
-#pragma unroll
-      for (int q = 0; q < NB; ++q) urow[q] = (lane < nbj && q >= lane && q < nbj) ? prow[q] : T(0);
 #pragma unroll
       for (int q = NB - 1; q >= 0; --q) {
         if (q < nbj) {
-          if (lane == q) y = y / urow[q];
+          if (lane == q) y = y / uv[q];
           const T xq = __shfl_sync(0xffffffffu, y, q);
-          if (lane < q) y = fma(-urow[q], xq, y);
+          if (lane < q) y = fma(-uv[q], xq, y);
         }
       }
       if (lane < nbj) sm.vsm[lane][c] = (double)y;
     }
     __syncthreads();
-    if (r < n) {
-      if (my_pos >= 0 && my_pos < J) {
-        T uv[NB];
-        load_row<T, NB>(row + J, nbj, uv);
+    if (upd) {
+      cp_async_wait<0>();
+      load_vec<T, NB>(seg, uv);
 #pragma unroll
-        for (int q = 0; q < NB; ++q)
-          if (q < nbj) {
+      for (int q = 0; q < NB; ++q)
+        if (q < nbj) {
 #pragma unroll
-            for (int c = 0; c < KK; ++c)
-              if (c < k) v[c] = fma(-uv[q], (T)sm.vsm[q][c], v[c]);
-          }
-      } else if (my_pos >= J && my_pos < J + nbj) {
+          for (int c = 0; c < KK; ++c)
+            if (c < k) v[c] = fma(-uv[q], (T)sm.vsm[q][c], v[c]);
+        }
+    } else if (r < n && my_pos >= J && my_pos < J + nbj) {
 #pragma unroll
-        for (int c = 0; c < KK; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
-      }
+      for (int c = 0; c < KK; ++c) v[c] = (T)sm.vsm[my_pos - J][c];
     }
     __syncthreads();
   }
@@ -603,16 +653,22 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
     rmax[c] = bmax[c] = 0.0;
     xmax[c] = tid < n ? fabs(sm.xs[tid][c]) : 0.0;
   }
+  // the lane's items of a row, all in flight before the first is used; the next row's are
+  // loaded while this one is reduced
+  double av[NMAX / 32];
+#pragma unroll
+  for (int q = 0; q < NMAX / 32; ++q)
+    av[q] = (warp < n && lane + 32 * q < n) ? __ldcs(a + (int64_t)warp * n + lane + 32 * q) : 0.0;
   for (int r = warp; r < n; r += WARPS) {
-    const double* ar = a + (int64_t)r * n;
     const double bv = lane < k ? b[(int64_t)r * k + lane] : 0.0;  // in flight beside the row
+    double nx[NMAX / 32];
+    const int rn = r + WARPS;
+#pragma unroll
+    for (int q = 0; q < NMAX / 32; ++q)
+      nx[q] = (rn < n && lane + 32 * q < n) ? __ldcs(a + (int64_t)rn * n + lane + 32 * q) : 0.0;
     double acc[KK], asum = 0.0;
 #pragma unroll
     for (int c = 0; c < KK; ++c) acc[c] = 0.0;
-    // the lane's items of the row, all in flight before the first is used
-    double av[NMAX / 32];
-#pragma unroll
-    for (int q = 0; q < NMAX / 32; ++q) av[q] = lane + 32 * q < n ? __ldg(ar + lane + 32 * q) : 0.0;
 #pragma unroll
     for (int q = 0; q < NMAX / 32; ++q) {
       const int j = lane + 32 * q;
@@ -645,6 +701,8 @@ __device__ double bresidual(const double* __restrict__ a, const double* __restri
           bmax[c] = fmax(bmax[c], fabs(bv));
         }
     }
+#pragma unroll
+    for (int q = 0; q < NMAX / 32; ++q) av[q] = nx[q];
   }
   // the lanes of a warp hold different columns: combine per warp, then across warps
 #pragma unroll
@@ -786,14 +844,7 @@ __device__ void solve_system(Batch& bt, Smem& sm, int n, int k, int nb, int ld, 
     __shared__ int irregular;
     if (threadIdx.x == 0) irregular = nonzero ? 0 : 1;
     __syncthreads();
-    double amax = 0.0;
-    for (int e = threadIdx.x; e < n * n; e += THREADS) amax = fmax(amax, fabs(a[e]));
-#pragma unroll
-    for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
-    if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5][0] = amax;
-    __syncthreads();
-    double big = 0.0;
-    for (int q = 0; q < WARPS; ++q) big = fmax(big, sm.red[q][0]);
+    const double big = sm.amax_a;  // from the load of this factorization
     if (my_pos >= 0) {
       const double u = W[(int64_t)threadIdx.x * ld + my_pos];
       if (fabs(u) <= DBL_EPSILON * n * big) atomicOr(&irregular, 1);
@@ -1131,14 +1182,7 @@ __global__ void __launch_bounds__(THREADS) batch_factor_kernel(const double* __r
   }
   for (int i = threadIdx.x; i < n; i += THREADS) perm[m * n + i] = sm.piv[i];
   if (regular) {
-    double amax = 0.0;
-    for (int e = threadIdx.x; e < n * n; e += THREADS) amax = fmax(amax, fabs(am[e]));
-#pragma unroll
-    for (int off = 16; off; off >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
-    if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5][0] = amax;
-    __syncthreads();
-    double big = 0.0;
-    for (int q = 0; q < WARPS; ++q) big = fmax(big, sm.red[q][0]);
+    const double big = sm.amax_a;
     if (my_pos >= 0 && fabs(W[(int64_t)threadIdx.x * ld + my_pos]) <= DBL_EPSILON * n * big) atomicOr(&irregular, 1);
     __syncthreads();
     if (threadIdx.x == 0) regular[m] = irregular ? 0 : 1;

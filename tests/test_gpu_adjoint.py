@@ -100,3 +100,25 @@ def test_gradcheck_small():
     b = torch.tensor(rng.standard_normal((3, 5, 2)), device="cuda", requires_grad=True)
     assert torch.autograd.gradcheck(lambda a, b: autograd.solve(a, b, method="plain"), (a, b), eps=1e-6,
                                     atol=1e-7, rtol=1e-6)
+
+
+def test_plans_are_reused_across_steps():
+    """A training loop of one shape builds its batch plan once (the plan cache), and each
+    step's gradients stay right."""
+    import torch
+    from rustymath_b200 import autograd
+    batch, n, k = 32, 20, 2
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    autograd._PLANS.clear()
+    for step in range(3):
+        a = (torch.randn(batch, n, n, generator=g, device="cuda", dtype=torch.float64) / 8
+             + torch.eye(n, device="cuda", dtype=torch.float64)).requires_grad_()
+        b = torch.randn(batch, n, k, generator=g, device="cuda", dtype=torch.float64).requires_grad_()
+        x = autograd.solve(a, b)
+        x.sum().backward()
+        want_b = torch.linalg.solve(a.detach().transpose(-1, -2), torch.ones_like(b))
+        assert torch.allclose(b.grad, want_b, rtol=1e-12, atol=1e-12)
+        assert torch.allclose(a.grad, -want_b @ x.detach().transpose(-1, -2), rtol=1e-11, atol=1e-11)
+    plans = [p for free in autograd._PLANS.values() for p in free]
+    assert len(plans) == 1

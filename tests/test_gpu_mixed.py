@@ -102,3 +102,20 @@ def test_mixed_without_fallback_reports_no_convergence(rb):
     st = _lib.load().rm_dsolve_host(n, a.ctypes.data, b.ctypes.data, k, x.ctypes.data, ctypes.byref(opts),
                                     ctypes.byref(rep))
     assert st == _lib.RM_NO_CONVERGENCE
+
+
+def test_window_without_a_good_pivot(rb):
+    """The mixed factorization pivots each 128-column panel among its own 256 rows. With the
+    first 256 rows scaled by 1e-8 the first panels find only tiny candidates in their window,
+    while the large entries sit below it: the float32 factors grow and classical refinement
+    cannot recover. The solve must still meet the float64 bar through one of its other routes
+    (GMRES-IR, or the plain float64 LU after fallback), and the report must say which."""
+    n, k = 1024, 3
+    a, b = conditioned(n, k, 1e2, 11)
+    a[:256] *= 1e-8
+    x, reps = rb.solve_report(a, b, method="mixed")
+    rep = reps[0]
+    assert rep.method_used in (0, 1, 2)
+    assert rep.fell_back == (1 if rep.method_used == 0 else 0)
+    assert O.backward_error(a, x, b) <= n * 2.0 ** -53
+    print(f"window test: method_used={rep.method_used} iterations={rep.iterations} fell_back={rep.fell_back}")
