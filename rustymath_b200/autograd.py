@@ -15,25 +15,33 @@ from .batched import BatchPlan
 __all__ = ["solve", "BatchedSolve"]
 
 # Plans (scratch, sorted order, captured graph) by (device, batch, n, k, method): a training
-# loop solving systems of one shape reuses its plan instead of building one per forward. The
-# forward's factors live in the plan until its backward has run, so a plan is lent to one
-# forward at a time; a second forward of the same shape before the first's backward gets a
-# plan of its own.
+# loop solving systems of one shape reuses its plans instead of building one per forward. A
+# forward's factors live in its plan until its graph is freed (backward may run more than once
+# on a retained graph), so a plan is leased to one forward's autograd node and comes back to
+# the cache when that node is freed; forwards whose nodes are alive at once get plans of their
+# own.
 _PLANS = {}
 
 
-def _plan(device, batch, n, k, method):
+class _Lease:
+    def __init__(self, key, plan):
+        self.key, self.plan = key, plan
+
+    def __del__(self):
+        try:
+            free = _PLANS.setdefault(self.key, [])
+            if len(free) < 4:
+                free.append(self.plan)
+                return
+        except Exception:  # interpreter shutdown: the cache may be gone already
+            pass
+        self.plan.close()
+
+
+def _lease(device, batch, n, k, method):
     key = (str(device), batch, n, k, method)
     free = _PLANS.setdefault(key, [])
-    return free.pop() if free else BatchPlan([n] * batch, [k] * batch, method=method), key
-
-
-def _release(key, plan):
-    free = _PLANS.setdefault(key, [])
-    if len(free) < 4:
-        free.append(plan)
-    else:
-        plan.close()
+    return _Lease(key, free.pop() if free else BatchPlan([n] * batch, [k] * batch, method=method))
 
 
 class BatchedSolve(torch.autograd.Function):
@@ -43,17 +51,17 @@ class BatchedSolve(torch.autograd.Function):
     def forward(ctx, a, b, method):
         batch, n, _ = a.shape
         k = b.shape[-1]
-        plan, key = _plan(a.device, batch, n, k, method)
+        lease = _lease(a.device, batch, n, k, method)
+        plan = lease.plan
         af = a.detach().contiguous().view(-1)
         bf = b.detach().contiguous().view(-1)
         x = torch.empty(batch * n * k, dtype=torch.float64, device=a.device)
         if batch:
             plan.execute(af, bf, x)
-        ctx.plan, ctx.key = plan, key
         ctx.shapes = (batch, n, k)
-        if not (ctx.needs_input_grad[0] or ctx.needs_input_grad[1]):
-            _release(key, plan)  # no backward will read the factors
-            ctx.plan = None
+        # the lease (and so the plan's factors) lives with the node; with no gradient wanted it
+        # goes back at once
+        ctx.lease = lease if (ctx.needs_input_grad[0] or ctx.needs_input_grad[1]) else None
         ctx.save_for_backward(af, x)
         return x.view(batch, n, k)
 
@@ -61,13 +69,11 @@ class BatchedSolve(torch.autograd.Function):
     def backward(ctx, gx):
         af, x = ctx.saved_tensors
         batch, n, k = ctx.shapes
-        plan = ctx.plan
+        plan = ctx.lease.plan
         gb = torch.empty(batch * n * k, dtype=torch.float64, device=x.device)
         ga = torch.empty(batch * n * n, dtype=torch.float64, device=x.device) if ctx.needs_input_grad[0] else None
         if batch:
             plan.adjoint(af, x, gx.detach().to(torch.float64).contiguous().view(-1), gb, ga)
-        _release(ctx.key, plan)
-        ctx.plan = None
         return (None if ga is None else ga.view(batch, n, n)), gb.view(batch, n, k), None
 
 

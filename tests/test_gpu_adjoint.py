@@ -120,5 +120,6 @@ def test_plans_are_reused_across_steps():
         want_b = torch.linalg.solve(a.detach().transpose(-1, -2), torch.ones_like(b))
         assert torch.allclose(b.grad, want_b, rtol=1e-12, atol=1e-12)
         assert torch.allclose(a.grad, -want_b @ x.detach().transpose(-1, -2), rtol=1e-11, atol=1e-11)
+        del x  # the step's graph goes, and its plan back to the cache
     plans = [p for free in autograd._PLANS.values() for p in free]
     assert len(plans) == 1
