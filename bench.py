@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm", "update", "small"],
                    help="single: the n=8192 system (the headline); batched: 20,000 uneven systems")
     p.add_argument("--count", type=int, default=20000, help="systems in the batched workload")
+    p.add_argument("--uniform-n", type=int, default=0,
+                   help="batched workload with every system of this order (a profiling case; 0: the U{8..256} mix)")
     return p.parse_args()
 
 
@@ -289,13 +291,16 @@ BATCH_WORKLOAD = ("20,000 systems, n~U{8..256}, nrhs~U{1..4} (numpy default_rng(
                   "(torch seeded generator on the GPU)")
 
 
-def make_batch(count, seed, device):
+def make_batch(count, seed, device, uniform_n=0):
     """Shapes from numpy's default_rng(seed) as the configuration states; entries from torch's
-    seeded generator on the GPU (same distributions): A = N(0,1) + n I, B = N(0,1)."""
+    seeded generator on the GPU (same distributions): A = N(0,1) + n I, B = N(0,1). uniform_n > 0
+    gives every system that order instead (for profiling one size)."""
     import torch
     rng = np.random.default_rng(seed)
     ns = rng.integers(8, 257, count)
     ks = rng.integers(1, 5, count)
+    if uniform_n:
+        ns[:] = uniform_n
     g = torch.Generator(device=device)
     g.manual_seed(seed)
     a = torch.randn(int((ns * ns).sum()), generator=g, device=device, dtype=torch.float64)
@@ -352,7 +357,7 @@ def run_batched(args, rank, world, local):
     import rustymath_b200 as rb
     from rustymath_b200 import _lib
     lib = _lib.load()
-    ns, ks, a, b = make_batch(args.count, 1 + rank, dev)
+    ns, ks, a, b = make_batch(args.count, 1 + rank, dev, args.uniform_n)
     x = torch.zeros(int((ns * ks).sum()), dtype=torch.float64, device=dev)
 
     def arm(method, steps, clocks=None):
@@ -400,7 +405,9 @@ def run_batched(args, rank, world, local):
     line = {"metric": BATCH_METRIC, "value": count / t, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": BATCH_WORKLOAD, "count": count, "panel_widths_by_bucket": widths,
+            "config": {"workload": BATCH_WORKLOAD if not args.uniform_n else
+                       f"{count} systems n={args.uniform_n}, nrhs~U{{1..4}}, A=N(0,1)+n*I (profiling case)",
+                       "count": count, "panel_widths_by_bucket": widths,
                        "l2": "inputs larger than L2 (A is %.1f GB)" % (a_bytes / 1e9)},
             "backward_error_max": rep.max_backward_error, "fell_back": rep.fell_back,
             "max_iterations": rep.max_iterations,

@@ -32,15 +32,21 @@ __global__ void __launch_bounds__(TB) invert_diag_blocks_kernel(const T* __restr
                                                                 T* __restrict__ dinv, bool lower_unit, bool upper_unit) {
   extern __shared__ uint8_t smraw[];
   T(*x)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(smraw);
+  T(*t)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(smraw + (size_t)TB * (TB + 1) * sizeof(T));
   const int b = blockIdx.x, which = blockIdx.y;  // 0: L, 1: U
   const int64_t r0 = (int64_t)b * TB;
   const int rows = (int)(n - r0 < TB ? n - r0 : TB);
   const T* blk = w + r0 * ldw + r0;
   const int col = threadIdx.x;
-  auto A = [&](int i, int j) -> T {
-    if (i >= rows || j >= rows) return i == j ? T(1) : T(0);
-    return COLMAJOR ? blk[(int64_t)j * ldw + i] : blk[(int64_t)i * ldw + j];
-  };
+  // the block in shared memory first (read along its storage order, coalesced); past n, identity
+  for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+    const int s0 = e / TB, s1 = e % TB;  // s1 runs along the storage
+    const int i = COLMAJOR ? s1 : s0, j = COLMAJOR ? s0 : s1;
+    t[i][j] = (i >= rows || j >= rows) ? (i == j ? T(1) : T(0))
+                                       : (COLMAJOR ? blk[(int64_t)j * ldw + i] : blk[(int64_t)i * ldw + j]);
+  }
+  __syncthreads();
+  auto A = [&](int i, int j) -> T { return t[i][j]; };
   if (which == 0) {
     // lower: x_i = (delta_i,col - sum_{col<=k<i} L_ik x_k) / L_ii for i >= col
     for (int i = 0; i < TB; ++i) {
@@ -126,10 +132,11 @@ template <typename T, bool COLMAJOR, int TB>
 static int launch_invert(const T* w, int64_t ldw, int64_t n, T* dinv, bool lower_unit, bool upper_unit,
                          cudaStream_t stream) {
   const size_t smem = (size_t)TB * (TB + 1) * sizeof(T);
-  RM_TRY(smem_attribute(invert_diag_blocks_kernel<T, COLMAJOR, TB>, smem));
+  RM_TRY(smem_attribute(invert_diag_blocks_kernel<T, COLMAJOR, TB>, 2 * smem));
   RM_TRY(smem_attribute(coupling_kernel<T, COLMAJOR, TB>, 2 * smem));
   dim3 grid((unsigned)((n + TB - 1) / TB), 2);
-  invert_diag_blocks_kernel<T, COLMAJOR, TB><<<grid, TB, smem, stream>>>(w, ldw, n, dinv, lower_unit, upper_unit);
+  invert_diag_blocks_kernel<T, COLMAJOR, TB><<<grid, TB, 2 * smem, stream>>>(w, ldw, n, dinv, lower_unit,
+                                                                              upper_unit);
   RM_LAUNCHED();
   if (grid.x > 1) {
     coupling_kernel<T, COLMAJOR, TB><<<grid, 256, 2 * smem, stream>>>(w, ldw, n, dinv);
