@@ -407,7 +407,7 @@ def run_batched(args, rank, world, local):
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": BATCH_WORKLOAD if not args.uniform_n else
                        f"{count} systems n={args.uniform_n}, nrhs~U{{1..4}}, A=N(0,1)+n*I (profiling case)",
-                       "count": count, "panel_widths_by_bucket": widths,
+                       "count": count, "panel_widths_by_bucket": widths, "cta_threads_by_bucket": plan.cta_threads(),
                        "l2": "inputs larger than L2 (A is %.1f GB)" % (a_bytes / 1e9)},
             "backward_error_max": rep.max_backward_error, "fell_back": rep.fell_back,
             "max_iterations": rep.max_iterations,
@@ -515,6 +515,37 @@ def run_adjoint(args, rank, world, local):
     t = (fwd + bwd) / args.steps
     berr, mx = plan.adjoint_results()
     da_bytes = batch * n * n * 8
+    # end to end through the public differentiable call: every step copies A, b and w in from
+    # pinned host memory, runs rustymath_b200.autograd.solve and loss.backward(), and copies
+    # dL/dA and dL/db back
+    from rustymath_b200 import autograd
+    a_h = a.view(batch, n, n).cpu().pin_memory()
+    b_h = b.view(batch, n, k).cpu().pin_memory()
+    w_h = w.view(batch, n, k).cpu().pin_memory()
+    ga_h = torch.empty(a_h.shape, dtype=torch.float64).pin_memory()
+    gb_h = torch.empty(b_h.shape, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        ad = a_h.to(dev, non_blocking=True).requires_grad_()
+        bd = b_h.to(dev, non_blocking=True).requires_grad_()
+        wd = w_h.to(dev, non_blocking=True)
+        (autograd.solve(ad, bd) * wd).sum().backward()
+        ga_h.copy_(ad.grad, non_blocking=True)
+        gb_h.copy_(bd.grad, non_blocking=True)
+        torch.cuda.synchronize()
+
+    for _ in range(2):
+        e2e_step()
+    e2e_steps = max(3, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_t = (time.perf_counter() - t0) / e2e_steps
+    assert torch.allclose(gb_h.view(-1).to(dev), gb) and torch.allclose(ga_h.view(-1).to(dev), ga)
+    e2e = {"value": batch / e2e_t, "unit": "systems/s (forward + backward)",
+           "h2d_bytes_per_step": (batch * n * n + 2 * batch * n * k) * 8,
+           "d2h_bytes_per_step": (batch * n * n + batch * n * k) * 8,
+           "api": "rustymath_b200.autograd.solve + loss.backward(), pinned copies"}
     line = {"metric": ADJ_METRIC, "value": batch / t, "unit": "systems/s (forward + backward)", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
@@ -525,7 +556,7 @@ def run_adjoint(args, rank, world, local):
                          "achieved": (2 * da_bytes) / (bwd / args.steps) / 1e9, "peak": peak_hbm(), "unit": "GB/s",
                          "frac": (2 * da_bytes) / (bwd / args.steps) / 1e9 / peak_hbm(), "traffic": None,
                          "note": "algorithmic bytes: A read once (transposed residual) + dA written once"},
-            "gpu_launches": launches, "clocks": clocks.summary()}
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary()}
     print(json.dumps(line, default=_jsonable), flush=True)
 
 

@@ -279,7 +279,8 @@ int rm_batch_plan_create(int64_t count, const int64_t *h_n, const int64_t *h_k, 
                          const int64_t *h_b_off, const int64_t *h_x_off, const rm_solve_options *opts,
                          rm_batch_plan **plan);
 /* Times each size bucket's candidate panel widths on these inputs (solving them) and keeps the
- * fastest; synchronises on `stream`. */
+ * fastest, then the CTA size (64 or 256 threads) for the systems of n <= 32 and n <= 64;
+ * synchronises on `stream`. */
 int rm_batch_plan_tune(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x, void *stream);
 /* One persistent kernel launch for all systems, replayed from a CUDA graph; asynchronous on
  * `stream`. */
@@ -302,6 +303,9 @@ int rm_batch_plan_adjoint(rm_batch_plan *plan, const double *d_a, const double *
 int rm_batch_plan_adjoint_results(rm_batch_plan *plan, double *h_berr, double *h_max_berr);
 /* The panel width chosen for size bucket 0..4 (n <= 32, 64, 128, 192, 256). */
 int rm_batch_plan_panel_width(const rm_batch_plan *plan, int bucket);
+/* The threads per CTA (a thread per row) that solve size bucket 0..4: 64 or 256 (the
+ * 64-thread build takes systems of n <= 64 unless the tuner chose otherwise). */
+int rm_batch_plan_cta_threads(const rm_batch_plan *plan, int bucket);
 int rm_batch_plan_destroy(rm_batch_plan *plan);
 /* create + execute + results + destroy; synchronises. RM_NO_CONVERGENCE when a system stalled
  * with fallback off. */

@@ -80,9 +80,15 @@ class BatchPlan:
                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
 
     def tune(self, a, b, x):
-        """Times the candidate panel widths per size bucket on these inputs; keeps the fastest."""
+        """Times the candidate panel widths per size bucket, and the CTA size for the systems of
+        n <= 64, on these inputs; keeps the fastest. Returns the panel widths per bucket."""
         check(_lib.load().rm_batch_plan_tune(self._h, *self._ptrs(a, b, x)), "batch tune")
         return [_lib.load().rm_batch_plan_panel_width(self._h, i) for i in range(5)]
+
+    def cta_threads(self):
+        """Threads per CTA (a thread per row: 64 or 256) solving each size bucket (n <= 32, 64,
+        128, 192, 256)."""
+        return [_lib.load().rm_batch_plan_cta_threads(self._h, i) for i in range(5)]
 
     def execute(self, a, b, x):
         """One persistent launch for every system (asynchronous on the current stream)."""

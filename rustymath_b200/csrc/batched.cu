@@ -56,7 +56,8 @@ struct BatchPlan {
   double* d_adj_berr = nullptr;
   unsigned char* d_w = nullptr;
   size_t w_bytes = 0;
-  int split = 0;  // items [0, split) (n > 64) go to the 256-thread kernel, the rest to the 64-thread one
+  int small_limit = bt64::MAX_N;  // the largest n the 64-thread build takes (64, 32 or 0; tuned)
+  int split = 0;  // items [0, split) (n > small_limit) go to the 256-thread kernel, the rest to the 64-thread one
   int grid = 0, grid_small = 0;
   cudaStream_t stream = nullptr;  // the plan's own stream, for graph capture
   cudaStream_t side = nullptr;    // the 64-thread kernel's, beside the other inside the graph
@@ -68,6 +69,7 @@ struct BatchPlan {
 };
 
 static int bucket_of(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : n <= 192 ? 3 : 4; }
+static constexpr int kBucketMax[5] = {32, 64, 128, 192, 256};
 
 static void free_plan(BatchPlan* p) {
   if (!p) return;
@@ -89,6 +91,12 @@ static int upload(V** dst, const std::vector<V>& src) {
   RM_CUDA_TRY(cudaMalloc(dst, std::max<size_t>(src.size(), 1) * sizeof(V)));
   if (!src.empty()) RM_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
   return RM_OK;
+}
+
+// the first item of the size-sorted order that the 64-thread build takes
+static void set_split(BatchPlan* p) {
+  p->split = 0;
+  while (p->split < (int)p->count && p->n[p->order[p->split]] > p->small_limit) ++p->split;
 }
 
 static int plan_build(BatchPlan* p) {
@@ -127,8 +135,7 @@ static int plan_build(BatchPlan* p) {
   RM_CUDA_TRY(cudaMalloc(&p->d_flags, std::max<int64_t>(cnt, 1) * sizeof(int)));
   RM_CUDA_TRY(cudaMalloc(&p->d_counter, 2 * sizeof(int)));  // one per kernel
   RM_CUDA_TRY(cudaMalloc(&p->d_w, p->w_bytes));
-  p->split = 0;
-  while (p->split < cnt && p->n[p->order[p->split]] > bt64::MAX_N) ++p->split;
+  set_split(p);
   int per_sm = 0, per_sm_small = 0;
   RM_TRY(bt::prepare(&per_sm));
   RM_TRY(bt64::prepare(&per_sm_small));
@@ -272,7 +279,9 @@ int batch_plan_execute(BatchPlan* p, const double* a, const double* b, double* x
 
 // Picks the panel width of each size bucket: each candidate (16, 32) runs the bucket's own
 // systems (a contiguous range of the size-sorted order) twice, timed by CUDA events; the
-// faster stays. The results are the solves of those systems (x is written).
+// faster stays. Then the CTA size for the systems of n <= 64: each choice of the largest n
+// that the 64-thread build takes (64, 32, or none: all on 256-thread CTAs) runs those systems
+// twice, and the fastest stays. The results are the solves of those systems (x is written).
 int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, cudaStream_t s) {
   if (!p) return RM_BAD_ARG;
   const int cnt = (int)p->count;
@@ -310,10 +319,37 @@ int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, c
                         cudaMemcpyHostToDevice, s) != cudaSuccess)
       status = RM_CUDA_ERROR;
   }
+  const int old_split = p->split;
+  int small_first = 0;
+  while (small_first < cnt && p->n[p->order[small_first]] > bt64::MAX_N) ++small_first;
+  if (status == RM_OK && small_first < cnt) {
+    float best = INFINITY;
+    int best_limit = p->small_limit;
+    for (int limit : {bt64::MAX_N, 32, 0}) {
+      p->small_limit = limit;
+      set_split(p);
+      float t = 0.0f;
+      for (int rep = 0; rep < 2 && status == RM_OK; ++rep) {
+        cudaEventRecord(e0, s);
+        status = launch_batch(p, a, b, x, small_first, cnt, s);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) status = RM_CUDA_ERROR;
+        cudaEventElapsedTime(&t, e0, e1);
+      }
+      if (t < best) best = t, best_limit = limit;
+    }
+    p->small_limit = best_limit;
+    set_split(p);
+  }
   cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  return status;  // the kernel reads the widths from d_nb, so a captured graph stays valid
+  // the kernels read the widths from d_nb, so a captured graph stays valid unless the split moved
+  if (p->split != old_split && p->graph) {
+    cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+  }
+  return status;
 }
 
 // dL/db = A^-T g and dL/dA = -(dL/db) x^T for every system, from the factors the last
@@ -437,6 +473,11 @@ int rm_batch_plan_adjoint_results(rm_batch_plan* plan, double* h_berr, double* h
 
 int rm_batch_plan_panel_width(const rm_batch_plan* plan, int bucket) {
   return plan && bucket >= 0 && bucket < 5 ? plan->p->nb_bucket[bucket] : 0;
+}
+
+int rm_batch_plan_cta_threads(const rm_batch_plan* plan, int bucket) {
+  if (!plan || bucket < 0 || bucket >= 5) return 0;
+  return rm::kBucketMax[bucket] <= plan->p->small_limit ? rm::bt64::MAX_N : rm::bt::MAX_N;
 }
 
 int rm_batch_plan_destroy(rm_batch_plan* plan) {

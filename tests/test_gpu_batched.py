@@ -132,8 +132,14 @@ def test_tune_and_graph_replay(rb):
     plan = rb.BatchPlan(sizes, ks, method="mixed")
     a, b = plan.pack(As, Bs, device="cuda")
     x = torch.zeros(plan.b_size, dtype=torch.float64, device="cuda")
+    assert plan.cta_threads() == [64, 64, 256, 256, 256]
     widths = plan.tune(a, b, x)
     assert all(w in (16, 32) for w in widths)
+    threads = plan.cta_threads()
+    assert threads[2:] == [256] * 3 and all(t in (64, 256) for t in threads[:2])
+    assert threads[0] == 64 or threads[1] == 256  # one split of the size-sorted order
+    # the tuner's last trial ran the systems of n <= 64 on 256-thread CTAs
+    check_bar(As, Bs, [t.cpu().numpy() for t in plan.unpack(x)])
     plan.execute(a, b, x)
     check_bar(As, Bs, [t.cpu().numpy() for t in plan.unpack(x)])
     # the same pointers replay the captured graph; new right-hand sides in place
