@@ -554,7 +554,9 @@ def run_adjoint(args, rank, world, local):
             "adjoint_backward_error_max": mx,
             "roofline": {"bound": "hbm", "kernel": "batch_adjoint_kernel",
                          "achieved": (2 * da_bytes) / (bwd / args.steps) / 1e9, "peak": peak_hbm(), "unit": "GB/s",
-                         "frac": (2 * da_bytes) / (bwd / args.steps) / 1e9 / peak_hbm(), "traffic": None,
+                         "frac": (2 * da_bytes) / (bwd / args.steps) / 1e9 / peak_hbm(), "traffic": 212.07e6 + 91.30e6,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the timed launch at "
+                                           "full size (profiles/batch_kernels_n64x4096.md)",
                          "note": "algorithmic bytes: A read once (transposed residual) + dA written once"},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary()}
     print(json.dumps(line, default=_jsonable), flush=True)

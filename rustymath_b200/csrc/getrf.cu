@@ -252,6 +252,132 @@ __global__ void __launch_bounds__(kPanelThreads)
   if (P > 1) cluster_sync_all();  // no CTA leaves while a peer may still read its memory
 }
 
+// ------------------------------------------------------------------ short leaves in one CTA
+// A leaf whose rows (M = n - j0) fit one CTA, a thread per row, factored from registers with
+// one CTA barrier per column. Rows do not move while the leaf is factored: each thread keeps
+// its row's current position (relative to j0), and a swap of positions d and p only exchanges
+// the two threads' positions; at the end every row is stored at its final position, which is
+// where the explicit swaps of panel_kernel would have put it. The arithmetic on every item is
+// panel_kernel's (the same reciprocal, the same fma per column in the same order), so the
+// results are the same bits; only the data movement differs.
+//
+// The pivot search per column: a candidate's key is its magnitude's bits + 1 (0 for NaN and
+// for rows already chosen); each warp finds its largest key and, among equal keys, the lowest
+// position (three redux.sync), and its winner posts its row, position, key and reciprocal;
+// after the barrier every warp reduces the posts the same way and reads the winning row.
+// When every candidate is NaN the pivot is the diagonal's row (factor.rs:476), posted after a
+// second barrier.
+constexpr int kShortLeafMaxRows = 512;
+constexpr int kShortWarps = kShortLeafMaxRows / 32;
+
+struct alignas(16) ShortPost {
+  double row[kLeaf];
+  unsigned long long key;
+  double rcp;
+  int pos;
+  int pad[3];
+};
+
+__device__ __forceinline__ void short_reduce(unsigned long long key, unsigned pos, unsigned long long& kmax,
+                                             unsigned& pmin, int& lane_of) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool tie = hi == mhi && lo == mlo;
+  pmin = __reduce_min_sync(0xffffffffu, tie ? pos : 0xffffffffu);
+  lane_of = __ffs(__ballot_sync(0xffffffffu, tie && pos == pmin)) - 1;
+  kmax = ((unsigned long long)mhi << 32) | mlo;
+}
+
+__device__ __forceinline__ void short_post(ShortPost& post, const double (&v)[kLeaf], int c, int pos,
+                                           unsigned long long key) {
+  double2* dst = reinterpret_cast<double2*>(post.row);
+#pragma unroll
+  for (int q = c / 2; q < kLeaf / 2; ++q) dst[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  const double pv = v[c];
+  post.rcp = fabs(pv) < 2.2250738585072014e-308 ? 0.0 : 1.0 / pv;
+  post.key = key;
+  post.pos = pos;
+}
+
+__global__ void __launch_bounds__(kShortLeafMaxRows, 1)
+    short_leaf_kernel(double* __restrict__ w, int64_t ldw, int n, int j0, int jb, int64_t* __restrict__ ipiv) {
+  __shared__ ShortPost post[2][kShortWarps + 1];  // a post per warp, and the diagonal's row
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int warps = blockDim.x >> 5;
+  const int M = n - j0;
+  double v[kLeaf];
+  const double* src = w + (int64_t)(j0 + t) * ldw + j0;
+  if (t < M && jb == kLeaf && (ldw & 1) == 0 && ((reinterpret_cast<uintptr_t>(w) & 15) == 0)) {
+#pragma unroll
+    for (int q = 0; q < kLeaf / 2; ++q) {
+      const double2 x = reinterpret_cast<const double2*>(src)[q];
+      v[2 * q] = x.x, v[2 * q + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int cc = 0; cc < kLeaf; ++cc) v[cc] = (t < M && cc < jb) ? src[cc] : 0.0;
+  }
+  int pos = t < M ? t : INT_MAX;  // the row's current position; rows past M take no part
+  bool active = t < M;
+#pragma unroll
+  for (int c = 0; c < kLeaf; ++c) {
+    if (c >= jb) break;
+    ShortPost* pp = post[c & 1];
+    const double a = fabs(v[c]);
+    const unsigned long long key =
+        (active && a == a) ? (unsigned long long)__double_as_longlong(a) + 1ull : 0ull;
+    unsigned long long kw;
+    unsigned pw;
+    int wl;
+    short_reduce(key, (unsigned)pos, kw, pw, wl);
+    if (lane == wl) short_post(pp[warp], v, c, pos, key);
+    __syncthreads();
+    // every warp reduces the posts: the largest key, the lowest position among equals
+    const unsigned long long k2 = lane < warps ? pp[lane].key : 0ull;
+    const unsigned p2 = lane < warps ? (unsigned)pp[lane].pos : 0xffffffffu;
+    unsigned long long kg;
+    unsigned pg;
+    int bw;
+    short_reduce(k2, p2, kg, pg, bw);
+    const ShortPost* win = &pp[bw];
+    if (kg == 0ull) {  // every candidate is NaN: the diagonal's row is the pivot row
+      if (pos == c) short_post(pp[kShortWarps], v, c, pos, 0ull);
+      __syncthreads();
+      win = &pp[kShortWarps];
+    }
+    const int p = win->pos;
+    const double pivot = win->row[c];
+    const double r = win->rcp;
+    if (pos == p) {
+      active = false;
+      pos = c;
+    } else if (pos == c) {
+      pos = p;
+    }
+    if (t == 0) ipiv[j0 + c] = j0 + p;
+    if (active && pivot != 0.0) {
+      const bool sub = fabs(pivot) < 2.2250738585072014e-308;
+      double l = v[c];
+      l = sub ? l / pivot : l * r;
+      v[c] = l;
+      const double2* pr = reinterpret_cast<const double2*>(win->row);
+#pragma unroll
+      for (int q = (c + 1) / 2; q < kLeaf / 2; ++q) {
+        const double2 u = pr[q];
+        if (2 * q > c && 2 * q < jb) v[2 * q] = fma(l, -u.x, v[2 * q]);
+        if (2 * q + 1 > c && 2 * q + 1 < jb) v[2 * q + 1] = fma(l, -u.y, v[2 * q + 1]);
+      }
+    }
+  }
+  if (t < M) {
+    double* dst = w + (int64_t)(j0 + pos) * ldw + j0;
+#pragma unroll
+    for (int cc = 0; cc < kLeaf; ++cc)
+      if (cc < jb) dst[cc] = v[cc];
+  }
+}
+
 // ------------------------------------------------------------------ swaps + unit-lower solve
 constexpr int kSwapCols = 16;      // columns per CTA
 constexpr int kSwapThreads = 256;
@@ -424,6 +550,13 @@ static int panel_cluster_limit() {
 template <typename T>
 static int launch_panel(T* w, int64_t ldw, int n, int j0, int jb, int64_t* ipiv, cudaStream_t stream) {
   const int M = n - j0;
+  if constexpr (sizeof(T) == 8) {
+    if (M <= kShortLeafMaxRows) {  // one CTA, a thread per row
+      short_leaf_kernel<<<1, (M + 31) / 32 * 32, 0, stream>>>(w, ldw, n, j0, jb, ipiv);
+      RM_LAUNCHED();
+      return RM_OK;
+    }
+  }
   const size_t sh = (sizeof(PanelShared<T>) + 15) / 16 * 16;
   const int rows_cap = (int)((kPanelSmemBudget - sh) / (kPanelStride * sizeof(T)));
   const int pmax = panel_cluster_limit<T>();
