@@ -58,6 +58,8 @@ __global__ void __launch_bounds__(C::THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
   const int ktiles = (k + C::BK - 1) / C::BK;
+  griddep_launch_dependents();
+  griddep_wait();  // the kernel before this one in the stream has completed
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::STAGES; ++s) {
@@ -204,8 +206,9 @@ static int launch_cfg(const double* a, int64_t lda, const double* b, int64_t ldb
   }
   RM_TRY(smem_attribute(dgemm_kernel<C>, C::SMEM));
   dim3 grid((n + C::BN - 1) / C::BN, (m + C::BM - 1) / C::BM);
-  dgemm_kernel<C><<<grid, C::THREADS, C::SMEM, stream>>>(ta, tb, c, ldc, m, n, k, alpha, beta, status);
-  RM_LAUNCHED();
+  RM_CUDA_TRY(launch_dependent(dgemm_kernel<C>, grid, dim3(C::THREADS), C::SMEM, stream, ta, tb, c, ldc, m, n, k, alpha,
+                               beta, status));
+  note_launch();
   return RM_OK;
 }
 

@@ -253,129 +253,200 @@ __global__ void __launch_bounds__(kPanelThreads)
 }
 
 // ------------------------------------------------------------------ short leaves in one CTA
-// A leaf whose rows (M = n - j0) fit one CTA, a thread per row, factored from registers with
-// one CTA barrier per column. Rows do not move while the leaf is factored: each thread keeps
-// its row's current position (relative to j0), and a swap of positions d and p only exchanges
-// the two threads' positions; at the end every row is stored at its final position, which is
-// where the explicit swaps of panel_kernel would have put it. The arithmetic on every item is
-// panel_kernel's (the same reciprocal, the same fma per column in the same order), so the
-// results are the same bits; only the data movement differs.
+// A leaf whose rows (M = n - j0 <= 768) fit one CTA: a thread per row, the leaf in shared
+// memory, factored in sub-leaves of 8 columns. Rows do not move while the leaf is factored:
+// each thread keeps its row's current position (relative to j0), a swap of positions d and p
+// only exchanges the two threads' positions, and at the end every row is stored at its final
+// position, which is where the explicit swaps of panel_kernel would have put it.
 //
-// The pivot search per column: a candidate's key is its magnitude's bits + 1 (0 for NaN and
-// for rows already chosen); each warp finds its largest key and, among equal keys, the lowest
-// position (three redux.sync), and its winner posts its row, position, key and reciprocal;
-// after the barrier every warp reduces the posts the same way and reads the winning row.
-// When every candidate is NaN the pivot is the diagonal's row (factor.rs:476), posted after a
-// second barrier.
-constexpr int kShortLeafMaxRows = 512;
+// Per sub-leaf, each thread holds its row's 8 items in registers and each column costs one CTA
+// barrier: a candidate's key is its magnitude's bits + 1 (0 for NaN and for rows already
+// chosen); each warp finds its largest key and, among equal keys, the lowest position (a
+// redux.sync of the keys' high words; when several lanes share the largest high word, two
+// more for the low words and the positions); its winner posts its sub-leaf row, position, key
+// and reciprocal (every candidate forms its reciprocal while the reduction runs); after the
+// barrier every warp reduces the posts the same way and reads the winning row. When every
+// candidate is NaN the pivot is the diagonal's row (factor.rs:476), posted after a second
+// barrier. After the sub-leaf, its pivot rows' later columns are solved against their unit
+// lower triangle (a thread per column) and the rows still unchosen take the rank-8 update.
+//
+// The arithmetic on every item is panel_kernel's: the same reciprocal, and per item the same
+// fma per pivot column in the same order (the deferred update applies the sub-leaf's columns
+// one fma at a time in column order; a zero pivot's column is skipped, as panel_kernel skips
+// it), so the results are the same bits. The sub-leaf loop is not unrolled: the kernel's code
+// stays in the instruction cache (a leaf fully unrolled over 32 columns was bound by
+// instruction fetch).
+constexpr int kShortLeafMaxRows = 768;
 constexpr int kShortWarps = kShortLeafMaxRows / 32;
+constexpr int kSub = 8;
+constexpr int kShortStride = kLeaf + 1;  // doubles per row in shared memory
 
 struct alignas(16) ShortPost {
-  double row[kLeaf];
+  double row[kSub];
   unsigned long long key;
   double rcp;
   int pos;
   int pad[3];
 };
 
-__device__ __forceinline__ void short_reduce(unsigned long long key, unsigned pos, unsigned long long& kmax,
-                                             unsigned& pmin, int& lane_of) {
-  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
-  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
-  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
-  const bool tie = hi == mhi && lo == mlo;
-  pmin = __reduce_min_sync(0xffffffffu, tie ? pos : 0xffffffffu);
-  lane_of = __ffs(__ballot_sync(0xffffffffu, tie && pos == pmin)) - 1;
-  kmax = ((unsigned long long)mhi << 32) | mlo;
+struct ShortShared {
+  ShortPost post[2][kShortWarps + 1];  // a post per warp, and the diagonal's row
+  double ub[kSub][kLeaf];              // the sub-leaf's pivot rows, later columns (U12)
+  int pv[kSub];                        // the thread (row) of each pivot of the sub-leaf
+  int pos[kShortLeafMaxRows];          // final positions
+};
+
+constexpr size_t short_leaf_smem(int rows) {
+  return (sizeof(ShortShared) + 15) / 16 * 16 + (size_t)rows * kShortStride * sizeof(double);
 }
 
-__device__ __forceinline__ void short_post(ShortPost& post, const double (&v)[kLeaf], int c, int pos,
-                                           unsigned long long key) {
+// The lane holding the warp's largest key, the lowest position among equal keys; `zero` when
+// every key is 0.
+__device__ __forceinline__ int short_reduce(unsigned long long key, unsigned pos, bool& zero) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned top = __ballot_sync(0xffffffffu, hi == mhi);
+  zero = false;
+  if (__popc(top) == 1) return __ffs(top) - 1;  // mhi > 0 here: at most one lane holds a key of 0
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool tie = hi == mhi && lo == mlo;
+  const unsigned pmin = __reduce_min_sync(0xffffffffu, tie ? pos : 0xffffffffu);
+  zero = mhi == 0u && mlo == 0u;
+  return __ffs(__ballot_sync(0xffffffffu, tie && pos == pmin)) - 1;
+}
+
+// 1 / pivot as the cluster panel forms it (0 for a subnormal pivot, which is divided by)
+__device__ __forceinline__ double short_rcp(double pv) {
+  return fabs(pv) < 2.2250738585072014e-308 ? 0.0 : __drcp_rn(pv);
+}
+
+__device__ __forceinline__ void short_post(ShortPost& post, const double (&p)[kSub], int i, int pos,
+                                           unsigned long long key, double rcp) {
   double2* dst = reinterpret_cast<double2*>(post.row);
 #pragma unroll
-  for (int q = c / 2; q < kLeaf / 2; ++q) dst[q] = make_double2(v[2 * q], v[2 * q + 1]);
-  const double pv = v[c];
-  post.rcp = fabs(pv) < 2.2250738585072014e-308 ? 0.0 : 1.0 / pv;
+  for (int q = i / 2; q < kSub / 2; ++q) dst[q] = make_double2(p[2 * q], p[2 * q + 1]);
+  post.rcp = rcp;
   post.key = key;
   post.pos = pos;
 }
 
 __global__ void __launch_bounds__(kShortLeafMaxRows, 1)
     short_leaf_kernel(double* __restrict__ w, int64_t ldw, int n, int j0, int jb, int64_t* __restrict__ ipiv) {
-  __shared__ ShortPost post[2][kShortWarps + 1];  // a post per warp, and the diagonal's row
+  extern __shared__ __align__(16) uint8_t smem[];
+  ShortShared& sh = *reinterpret_cast<ShortShared*>(smem);
+  double* S = reinterpret_cast<double*>(smem + (sizeof(ShortShared) + 15) / 16 * 16);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int warps = blockDim.x >> 5;
   const int M = n - j0;
-  double v[kLeaf];
-  const double* src = w + (int64_t)(j0 + t) * ldw + j0;
-  if (t < M && jb == kLeaf && (ldw & 1) == 0 && ((reinterpret_cast<uintptr_t>(w) & 15) == 0)) {
-#pragma unroll
-    for (int q = 0; q < kLeaf / 2; ++q) {
-      const double2 x = reinterpret_cast<const double2*>(src)[q];
-      v[2 * q] = x.x, v[2 * q + 1] = x.y;
-    }
-  } else {
-#pragma unroll
-    for (int cc = 0; cc < kLeaf; ++cc) v[cc] = (t < M && cc < jb) ? src[cc] : 0.0;
-  }
-  int pos = t < M ? t : INT_MAX;  // the row's current position; rows past M take no part
+  griddep_launch_dependents();
+  griddep_wait();  // the kernel before this one in the stream has completed
+  // the leaf into shared memory: a warp per row, lanes along it (coalesced)
+  for (int r = warp; r < M; r += warps)
+    if (lane < jb) S[r * kShortStride + lane] = w[(int64_t)(j0 + r) * ldw + j0 + lane];
+  __syncthreads();
+  double* row = S + t * kShortStride;
+  int pos = t < M ? t : INT_MAX;  // the row's current position; threads past M take no part
   bool active = t < M;
+#pragma unroll 1
+  for (int c0 = 0; c0 < jb; c0 += kSub) {
+    double p[kSub];
 #pragma unroll
-  for (int c = 0; c < kLeaf; ++c) {
-    if (c >= jb) break;
-    ShortPost* pp = post[c & 1];
-    const double a = fabs(v[c]);
-    const unsigned long long key =
-        (active && a == a) ? (unsigned long long)__double_as_longlong(a) + 1ull : 0ull;
-    unsigned long long kw;
-    unsigned pw;
-    int wl;
-    short_reduce(key, (unsigned)pos, kw, pw, wl);
-    if (lane == wl) short_post(pp[warp], v, c, pos, key);
-    __syncthreads();
-    // every warp reduces the posts: the largest key, the lowest position among equals
-    const unsigned long long k2 = lane < warps ? pp[lane].key : 0ull;
-    const unsigned p2 = lane < warps ? (unsigned)pp[lane].pos : 0xffffffffu;
-    unsigned long long kg;
-    unsigned pg;
-    int bw;
-    short_reduce(k2, p2, kg, pg, bw);
-    const ShortPost* win = &pp[bw];
-    if (kg == 0ull) {  // every candidate is NaN: the diagonal's row is the pivot row
-      if (pos == c) short_post(pp[kShortWarps], v, c, pos, 0ull);
+    for (int i = 0; i < kSub; ++i) p[i] = (t < M && c0 + i < jb) ? row[c0 + i] : 0.0;
+    unsigned skip = 0;  // the sub-leaf's columns whose pivot was zero (left unreduced)
+#pragma unroll
+    for (int i = 0; i < kSub; ++i) {
+      const int c = c0 + i;
+      if (c >= jb) break;
+      ShortPost* pp = sh.post[c & 1];
+      const double a = fabs(p[i]);
+      const unsigned long long key =
+          (active && a == a) ? (unsigned long long)__double_as_longlong(a) + 1ull : 0ull;
+      const double myr = short_rcp(p[i]);
+      bool none;
+      const int wl = short_reduce(key, (unsigned)pos, none);
+      if (lane == wl) short_post(pp[warp], p, i, pos, key, myr);
       __syncthreads();
-      win = &pp[kShortWarps];
-    }
-    const int p = win->pos;
-    const double pivot = win->row[c];
-    const double r = win->rcp;
-    if (pos == p) {
-      active = false;
-      pos = c;
-    } else if (pos == c) {
-      pos = p;
-    }
-    if (t == 0) ipiv[j0 + c] = j0 + p;
-    if (active && pivot != 0.0) {
-      const bool sub = fabs(pivot) < 2.2250738585072014e-308;
-      double l = v[c];
-      l = sub ? l / pivot : l * r;
-      v[c] = l;
-      const double2* pr = reinterpret_cast<const double2*>(win->row);
+      // every warp reduces the posts: the largest key, the lowest position among equals
+      const unsigned long long k2 = lane < warps ? pp[lane].key : 0ull;
+      const unsigned p2 = lane < warps ? (unsigned)pp[lane].pos : 0xffffffffu;
+      const int bw = short_reduce(k2, p2, none);
+      const ShortPost* win = &pp[bw];
+      if (none) {  // every candidate is NaN: the diagonal's row is the pivot row
+        if (pos == c) short_post(pp[kShortWarps], p, i, pos, 0ull, myr);
+        __syncthreads();
+        win = &pp[kShortWarps];
+      }
+      const int pr = win->pos;
+      const double pivot = win->row[i];
+      const double r = win->rcp;
+      if (pos == pr) {
+        active = false;
+        pos = c;
+        sh.pv[i] = t;
+      } else if (pos == c) {
+        pos = pr;
+      }
+      if (t == 0) ipiv[j0 + c] = j0 + pr;
+      if (pivot == 0.0) skip |= 1u << i;
+      if (active && pivot != 0.0) {
+        const bool sub = fabs(pivot) < 2.2250738585072014e-308;
+        double l = p[i];
+        l = sub ? l / pivot : l * r;
+        p[i] = l;
+        const double2* prow = reinterpret_cast<const double2*>(win->row);
 #pragma unroll
-      for (int q = (c + 1) / 2; q < kLeaf / 2; ++q) {
-        const double2 u = pr[q];
-        if (2 * q > c && 2 * q < jb) v[2 * q] = fma(l, -u.x, v[2 * q]);
-        if (2 * q + 1 > c && 2 * q + 1 < jb) v[2 * q + 1] = fma(l, -u.y, v[2 * q + 1]);
+        for (int q = (i + 1) / 2; q < kSub / 2; ++q) {
+          const double2 u = prow[q];
+          if (2 * q > i) p[2 * q] = fma(l, -u.x, p[2 * q]);
+          if (2 * q + 1 > i) p[2 * q + 1] = fma(l, -u.y, p[2 * q + 1]);
+        }
       }
     }
-  }
-  if (t < M) {
-    double* dst = w + (int64_t)(j0 + pos) * ldw + j0;
+    if (t < M) {
 #pragma unroll
-    for (int cc = 0; cc < kLeaf; ++cc)
-      if (cc < jb) dst[cc] = v[cc];
+      for (int i = 0; i < kSub; ++i)
+        if (c0 + i < jb) row[c0 + i] = p[i];
+    }
+    const int rc0 = c0 + kSub, rcols = jb - rc0;
+    if (rcols <= 0) break;
+    __syncthreads();
+    // U12: the sub-leaf's pivot rows, later columns, against their unit lower triangle; a
+    // thread per column, the same fmas in the same order as the rank-1 updates
+    if (t < rcols) {
+      double u[kSub];
+#pragma unroll
+      for (int k = 0; k < kSub; ++k) u[k] = S[sh.pv[k] * kShortStride + rc0 + t];
+#pragma unroll
+      for (int k = 1; k < kSub; ++k) {
+        const double* lrow = S + sh.pv[k] * kShortStride + c0;
+#pragma unroll
+        for (int q = 0; q < k; ++q)
+          if (!((skip >> q) & 1u)) u[k] = fma(lrow[q], -u[q], u[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kSub; ++k) {
+        S[sh.pv[k] * kShortStride + rc0 + t] = u[k];
+        sh.ub[k][t] = u[k];
+      }
+    }
+    __syncthreads();
+    // the rows still unchosen: later columns, one fma per pivot column in column order
+    if (active) {
+      for (int j = 0; j < rcols; ++j) {
+        double x = row[rc0 + j];
+#pragma unroll
+        for (int k = 0; k < kSub; ++k)
+          if (!((skip >> k) & 1u)) x = fma(p[k], -sh.ub[k][j], x);
+        row[rc0 + j] = x;
+      }
+    }
+    __syncthreads();
   }
+  // the leaf back, every row at its final position: a warp per row, lanes along it
+  if (t < M) sh.pos[t] = pos;
+  __syncthreads();
+  for (int r2 = warp; r2 < M; r2 += warps)
+    if (lane < jb) w[(int64_t)(j0 + sh.pos[r2]) * ldw + j0 + lane] = S[r2 * kShortStride + lane];
 }
 
 // ------------------------------------------------------------------ swaps + unit-lower solve
@@ -397,6 +468,8 @@ __global__ void __launch_bounds__(kSwapThreads)
   __shared__ T lblk[kLeaf][kLeaf + 1];
   __shared__ int ipv[kMaxSwaps];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  griddep_launch_dependents();
+  griddep_wait();  // the kernel before this one in the stream has completed
   // the swaps' targets, all at once (the loop below is sequential over them)
   for (int q = tid; q < jb; q += kSwapThreads) ipv[q] = (int)ipiv[j0 + q];
   __syncthreads();
@@ -552,8 +625,10 @@ static int launch_panel(T* w, int64_t ldw, int n, int j0, int jb, int64_t* ipiv,
   const int M = n - j0;
   if constexpr (sizeof(T) == 8) {
     if (M <= kShortLeafMaxRows) {  // one CTA, a thread per row
-      short_leaf_kernel<<<1, (M + 31) / 32 * 32, 0, stream>>>(w, ldw, n, j0, jb, ipiv);
-      RM_LAUNCHED();
+      RM_TRY(smem_attribute(short_leaf_kernel, short_leaf_smem(kShortLeafMaxRows)));
+      RM_CUDA_TRY(launch_dependent(short_leaf_kernel, dim3(1), dim3((M + 31) / 32 * 32), short_leaf_smem(M), stream, w,
+                                   ldw, n, j0, jb, ipiv));
+      note_launch();
       return RM_OK;
     }
   }
@@ -597,9 +672,9 @@ static int launch_swap(T* w, int64_t ldw, int j0, int jb, const int64_t* ipiv, i
   const int chunks = (hi1 - lo1 + kSwapCols - 1) / kSwapCols + (hi2 - lo2 + kSwapCols - 1) / kSwapCols;
   const int grid = max(chunks, perm ? 1 : 0);
   if (grid == 0) return RM_OK;
-  swap_trsm_kernel<T><<<grid, kSwapThreads, 0, stream>>>(w, ldw, j0, jb, ipiv, lo1, hi1, lo2, hi2, trsm_lo, trsm_hi,
-                                                           perm);
-  RM_LAUNCHED();
+  RM_CUDA_TRY(launch_dependent(swap_trsm_kernel<T>, dim3(grid), dim3(kSwapThreads), 0, stream, w, ldw, j0, jb, ipiv, lo1,
+                               hi1, lo2, hi2, trsm_lo, trsm_hi, perm));
+  note_launch();
   return RM_OK;
 }
 
@@ -622,6 +697,8 @@ __global__ void __launch_bounds__(256) invert_unit_lower_f64_kernel(const double
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ab = blockIdx.x, a0 = kLeaf * ab;
   const double* l = w + (int64_t)j0 * ldw + j0;
+  griddep_launch_dependents();
+  griddep_wait();  // the kernel before this one in the stream has completed
   // L from row and column a0 on (strictly lower part; unit diagonal implied)
   for (int i = a0 + warp; i < kOuter; i += 8)
     for (int k = a0 + lane; k < kOuter; k += 32) M[i][k] = (i < nb && k < nb && k < i) ? l[(int64_t)i * ldw + k] : 0.0;
@@ -741,8 +818,9 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
     if (ahead && J0 > 0) RM_CUDA_TRY(cudaStreamWaitEvent(stream, la.rest_done, 0));
     RM_TRY(launch_swap<double>(w, ldw, J0, nb, ipiv, 0, J0, J1, n, 0, 0, perm, stream));
     if (J1 < n) {
-      invert_unit_lower_f64_kernel<<<kOuter / kLeaf, 256, kInv64Smem, stream>>>(w, ldw, J0, nb, linv);
-      RM_LAUNCHED();
+      RM_CUDA_TRY(launch_dependent(invert_unit_lower_f64_kernel, dim3(kOuter / kLeaf), dim3(256), kInv64Smem, stream,
+                                   (const double*)w, ldw, J0, nb, linv));
+      note_launch();
       double* a12 = w + (int64_t)J0 * ldw + J1;
       RM_TRY(dgemm_device(false, false, nb, n - J1, nb, 1.0, linv, kOuter, a12, ldw, 0.0, a12, ldw, status, stream,
                           /*force_wide_m=*/true));
