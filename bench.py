@@ -291,6 +291,17 @@ BATCH_WORKLOAD = ("20,000 systems, n~U{8..256}, nrhs~U{1..4} (numpy default_rng(
                   "(torch seeded generator on the GPU)")
 
 
+# DRAM bytes (read + write) that ncu measured for the timed mixed launch over the first 2,000
+# systems of the batched configuration (shapes from default_rng(1)); traffic grows with the
+# systems' sum of n^2, so the full batch's is estimated from it
+BATCH_TRAFFIC_2000 = 1522427904 + 282152448
+
+
+def batch_traffic_estimate(ns):
+    ref = np.random.default_rng(1).integers(8, 257, 2000).astype(np.int64)
+    return BATCH_TRAFFIC_2000 * float((np.asarray(ns, np.int64) ** 2).sum()) / float((ref ** 2).sum())
+
+
 def make_batch(count, seed, device, uniform_n=0):
     """Shapes from numpy's default_rng(seed) as the configuration states; entries from torch's
     seeded generator on the GPU (same distributions): A = N(0,1) + n I, B = N(0,1). uniform_n > 0
@@ -413,9 +424,14 @@ def run_batched(args, rank, world, local):
             "max_iterations": rep.max_iterations,
             "plain_fp64": {"solves_per_s": count / t_plain, "ms_per_step": 1e3 * t_plain,
                            "backward_error_max": rep_plain.max_backward_error},
-            "roofline": {"bound": "hbm", "kernel": "batch_solve_kernel (whole batch, one launch)",
+            "roofline": {"bound": "hbm", "kernel": "batch_solve_kernel (whole batch; the n <= 64 systems on a "
+                                                 "second launch beside it when the tuner keeps them there)",
                          "achieved": passes * a_bytes / t / 1e9, "peak": peak_hbm(), "unit": "GB/s",
-                         "frac": passes * a_bytes / t / 1e9 / peak_hbm(), "traffic": None,
+                         "frac": passes * a_bytes / t / 1e9 / peak_hbm(),
+                         "traffic": batch_traffic_estimate(ns),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the timed mixed launch "
+                                           "on the first 2,000 systems of this configuration (1.80 GB), scaled by "
+                                           "sum(n^2) to these systems (profiles/batch_solve_kernel_n256x1000.md)",
                          "note": "algorithmic bytes: A read once to factor plus once per residual"},
             "e2e": {"value": count / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": a_bytes + int(b.numel()) * 8,
                     "d2h_bytes_per_step": int(x.numel()) * 8, "api": "BatchPlan.execute + pinned copies"},
