@@ -641,6 +641,7 @@ def run_gemm(args, rank, world, local):
     clocks = ClockSampler(local)
     t_oz, e_oz, launches = timed(ozaki, steps, clocks)
     fl = 2.0 * n ** 3
+    gemv = gemv_legs(torch, lib, a, dev, max(3, steps))
     cross = gemm_cross_check(torch, lib, dev) if not args.no_cpu_baseline else None
     line = {"metric": GEMM_METRIC, "value": fl / t_oz / 1e12, "unit": "TFLOP/s (FP64-equivalent)", "n_gpus": world,
             "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_oz, "higher_is_better": True,
@@ -650,9 +651,43 @@ def run_gemm(args, rank, world, local):
             "max_rel_error_vs_|A||B|": {"ozaki": e_oz, "native_fp64": e_nat, "cublas_fp64": e_cub},
             "native_fp64": {"tflops": fl / t_nat / 1e12, "ms": 1e3 * t_nat},
             "cublas_fp64": {"tflops": fl / t_cub / 1e12, "ms": 1e3 * t_cub},
-            "cross_check_2048_vs_oracle": cross,
+            "cross_check_2048_vs_oracle": cross, "gemv": gemv,
             "gpu_launches": int(launches), "clocks": clocks.summary()}
     print(json.dumps(line, default=_jsonable), flush=True)
+
+
+def gemv_legs(torch, lib, a, dev, steps):
+    """y = A x and y = A^T x through rm_dgemm (n = 1: by_vector's shapes, the HBM-bound stream
+    kernels) on the n x n operand A of the GEMM legs (larger than L2): GB/s of A read per call
+    (CUDA events) against the measured copy bandwidth, and the largest difference from cuBLAS's
+    product relative to |A||x|."""
+    from rustymath_b200 import _lib
+    n = a.shape[0]
+    x = torch.rand(n, 1, device=dev, dtype=torch.float64) * 2 - 1
+    y = torch.empty(n, 1, device=dev, dtype=torch.float64)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {"workload": f"A {n}x{n} float64 ({8 * n * n / 1e9:.1f} GB), x ~ U(-1,1)", "peak_gbs": peak_hbm()}
+    for name, ta in (("a_x", 0), ("at_x", 1)):
+        def call():
+            _lib.check(lib.rm_dgemm(ta, 0, n, 1, n, 1.0, a.data_ptr(), n, x.data_ptr(), 1, 0.0, y.data_ptr(), 1, sp),
+                       "gemv")
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            call()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / steps
+        op = a.T if ta else a
+        ref = op @ x
+        mag = op.abs() @ x.abs()
+        gbs = 8.0 * n * n / t / 1e9
+        out[name] = {"ms": 1e3 * t, "gbs": gbs, "frac": gbs / peak_hbm(),
+                     "max_rel_diff_vs_cublas": float(((y - ref).abs() / mag).max())}
+    return out
 
 
 def gemm_cross_check(torch, lib, dev, n=2048, seed=5):

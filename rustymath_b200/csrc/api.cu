@@ -412,6 +412,8 @@ int rm_dgemm(int transa, int transb, int64_t m, int64_t n, int64_t k, double alp
   RM_TRY(check_device());
   cudaStream_t s = as_stream(stream);
   if (k == 0 || alpha == 0.0) return scale_device(d_c, ldc, m, n, beta, s);
+  // one output row or column: by_vector's case (linalg.rs:1020-1073), an HBM-bound stream
+  if (m == 1 || n == 1) return gemv_device(transa, transb, m, n, k, alpha, d_a, lda, d_b, ldb, beta, d_c, ldc, s);
   // TMA wants 16-byte aligned rows: copy misaligned operands into padded buffers.
   const double* a = d_a;
   const double* b = d_b;

@@ -15,6 +15,10 @@ int dgemm_device(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha
                  const double* b, int64_t ldb, double beta, double* c, int64_t ldc, unsigned* status,
                  cudaStream_t stream, bool force_wide_m = false);
 int scale_device(double* c, int64_t ldc, int64_t m, int64_t n, double beta, cudaStream_t stream);
+// C = alpha op(A) op(B) + beta C for m == 1 or n == 1 (k >= 1, alpha != 0): streams over the
+// matrix operand instead of DMMA tiles (gemv.cu)
+int gemv_device(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* a, int64_t lda,
+                const double* b, int64_t ldb, double beta, double* c, int64_t ldc, cudaStream_t stream);
 
 // ---------------------------------------------------------------- FP32 tensor-core GEMM (sgemm_tc.cu)
 // C = alpha A B^T + beta C in float32 on tcgen05: A m x k and B n x k row-major (k
