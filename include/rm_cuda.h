@@ -285,6 +285,14 @@ int rm_batch_plan_tune(rm_batch_plan *plan, const double *d_a, const double *d_b
 /* One persistent kernel launch for all systems, replayed from a CUDA graph; asynchronous on
  * `stream`. */
 int rm_batch_plan_execute(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x, void *stream);
+/* rm_batch_plan_execute from host memory: copies h_a and h_b (packed as for execute) into d_a
+ * and d_b, solves, and copies x back into h_x, in groups of consecutive systems so that one
+ * group's copies overlap another's solves (h_a, h_b, h_x pinned for the overlap). A plan whose
+ * offsets do not follow the systems' order takes one group. Asynchronous on `stream`: h_x holds
+ * the solutions once `stream` reaches the end. The results and the adjoint read it as an
+ * execute. (rustymath has no host-to-device path; this is the host-memory form of the stack.) */
+int rm_batch_plan_execute_host(rm_batch_plan *plan, const double *h_a, const double *h_b, double *h_x, double *d_a,
+                               double *d_b, double *d_x, void *stream);
 /* Per-system backward errors, refinement steps and RM_BATCH_* flags of the last execute (any
  * pointer may be NULL); synchronises. */
 int rm_batch_plan_results(rm_batch_plan *plan, double *h_berr, int32_t *h_iters, int32_t *h_flags,

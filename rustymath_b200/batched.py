@@ -94,6 +94,21 @@ class BatchPlan:
         """One persistent launch for every system (asynchronous on the current stream)."""
         check(_lib.load().rm_batch_plan_execute(self._h, *self._ptrs(a, b, x)), "batch execute")
 
+    def execute_host(self, a_h, b_h, x_h, a, b, x):
+        """execute from host memory: copies the CPU tensors a_h, b_h (pinned, for the copies to
+        overlap the solves) into the CUDA tensors a, b, solves, and copies x back into x_h, group
+        by group; asynchronous on the current stream (x_h is complete once it synchronises)."""
+        torch = _torch()
+        for t in (a_h, b_h, x_h):
+            if not (_is_torch(t) and not t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("execute_host takes contiguous float64 CPU tensors")
+        if a_h.numel() < self.a_size or b_h.numel() < self.b_size or x_h.numel() < self.b_size:
+            raise ValueError("the packed host arrays are smaller than the plan's shapes")
+        pa, pb, px, s = self._ptrs(a, b, x)
+        check(_lib.load().rm_batch_plan_execute_host(self._h, ctypes.c_void_p(a_h.data_ptr()),
+                                                     ctypes.c_void_p(b_h.data_ptr()), ctypes.c_void_p(x_h.data_ptr()),
+                                                     pa, pb, px, s), "batch execute_host")
+
     def adjoint(self, a, x, gx, gb, ga=None):
         """gb = A^-T gx and (unless ga is None) ga = -gb x^T for every system, from the factors
         of the last execute (a and x must be that execute's); asynchronous."""

@@ -66,6 +66,16 @@ struct BatchPlan {
   const void* g_b = nullptr;
   const void* g_x = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join = nullptr;
+  // execute_host: the systems in groups of consecutive indices (about equal bytes of A), each
+  // group's items sorted by size; built on the first call and again after a tune
+  int tune_gen = 0, groups_gen = -1;
+  std::vector<int> g_first;  // group g: items [g_first[g], g_first[g + 1]) of g_order
+  std::vector<int> g_split;  // its first item of n <= small_limit
+  std::vector<int> g_order, g_nb;
+  int *d_gsys = nullptr, *d_gnb = nullptr;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> g_in, g_done;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
 };
 
 static int bucket_of(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : n <= 192 ? 3 : 4; }
@@ -79,10 +89,14 @@ static void free_plan(BatchPlan* p) {
                   (void*)p->d_woff, (void*)p->d_berr, (void*)p->d_w, (void*)p->d_poff, (void*)p->d_piv,
                   (void*)p->d_ftype, (void*)p->d_adj_berr})
     if (q) cudaFree(q);
-  for (cudaEvent_t e : {p->ev_in, p->ev_out, p->ev_fork, p->ev_join})
+  for (cudaEvent_t e : {p->ev_in, p->ev_out, p->ev_fork, p->ev_join, p->ev_start, p->ev_end})
     if (e) cudaEventDestroy(e);
-  if (p->stream) cudaStreamDestroy(p->stream);
-  if (p->side) cudaStreamDestroy(p->side);
+  for (cudaEvent_t e : p->g_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->g_done) cudaEventDestroy(e);
+  if (p->d_gsys) cudaFree(p->d_gsys);
+  if (p->d_gnb) cudaFree(p->d_gnb);
+  for (cudaStream_t q : {p->stream, p->side, p->copy_in, p->copy_out})
+    if (q) cudaStreamDestroy(q);
   delete p;
 }
 
@@ -165,15 +179,16 @@ static BatchArgs batch_args(BatchPlan* p, const double* a, const double* b, doub
 }
 
 // Runs big(first, last, stream) over the items [first, last) ∩ [0, split) and small(...) over
-// [first, last) ∩ [split, count), after the counters' reset on s (counting the launches in
+// [first, last) ∩ [split, ...), after the counters' reset on s (counting the launches in
 // rm_launch_count when `count`). When both have items, the
 // 64-thread kernel runs on the plan's side stream, forked from s and joined back, so that its
 // CTAs fill the SMs that the 256-thread kernel's CTAs leave at its end; inside a capture the
 // fork and join become the graph's edges.
 template <typename Big, typename Small>
-static int launch_split(BatchPlan* p, int first, int last, cudaStream_t s, bool count, Big&& big, Small&& small) {
+static int launch_split(BatchPlan* p, int first, int last, int split, cudaStream_t s, bool count, Big&& big,
+                        Small&& small) {
   RM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 2 * sizeof(int), s));
-  const int b1 = std::min(last, p->split), s0 = std::max(first, p->split);
+  const int b1 = std::min(last, split), s0 = std::max(first, split);
   const bool has_big = first < b1, has_small = s0 < last;
   cudaStream_t ss = s;
   if (has_big && has_small) {
@@ -203,7 +218,7 @@ static int launch_split(BatchPlan* p, int first, int last, cudaStream_t s, bool 
 static int launch_batch(BatchPlan* p, const double* a, const double* b, double* x, int first, int last,
                         cudaStream_t s, bool captured = false) {
   RM_TRY(launch_split(
-      p, first, last, s, !captured,
+      p, first, last, p->split, s, !captured,
       [&](int f, int l, cudaStream_t st) {
         bt::launch_solve(batch_args(p, a, b, x, f, l, p->d_counter), std::min(p->grid, l - f), st);
       },
@@ -344,12 +359,134 @@ int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, c
   cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  ++p->tune_gen;  // execute_host rebuilds its groups with the new widths and split
   // the kernels read the widths from d_nb, so a captured graph stays valid unless the split moved
   if (p->split != old_split && p->graph) {
     cudaGraphExecDestroy(p->graph);
     p->graph = nullptr;
   }
   return status;
+}
+
+// ------------------------------------------------------------------ execute from host memory
+// The systems in groups of consecutive indices with about equal bytes of A (one group when the
+// packed offsets do not follow the indices), each group's items sorted by size, largest first,
+// with their panel widths and the first item of the 64-thread kernel.
+constexpr int kHostGroups = 6;
+
+static bool packed_in_order(const BatchPlan* p) {
+  for (int64_t i = 0; i + 1 < p->count; ++i) {
+    const int64_t n = p->n[i], k = p->k[i];
+    if (p->a_off[i + 1] < p->a_off[i] + n * n || p->b_off[i + 1] < p->b_off[i] + n * k ||
+        p->x_off[i + 1] < p->x_off[i] + n * k)
+      return false;
+  }
+  return true;
+}
+
+static int build_groups(BatchPlan* p) {
+  const int cnt = (int)p->count;
+  std::vector<int> bounds = {0};
+  if (cnt > 1 && packed_in_order(p)) {
+    int64_t total = 0, acc = 0;
+    for (int i = 0; i < cnt; ++i) total += (int64_t)p->n[i] * p->n[i];
+    const int G = std::min(kHostGroups, cnt);
+    int g = 1;
+    for (int i = 0; i + 1 < cnt && g < G; ++i) {
+      acc += (int64_t)p->n[i] * p->n[i];
+      if (acc * G >= total * g) bounds.push_back(i + 1), ++g;
+    }
+  }
+  bounds.push_back(cnt);
+  const int G = (int)bounds.size() - 1;
+  p->g_order.resize(cnt);
+  p->g_nb.resize(cnt);
+  p->g_first.assign(bounds.begin(), bounds.end());
+  p->g_split.assign(G, 0);
+  for (int g = 0; g < G; ++g) {
+    auto b = p->g_order.begin() + bounds[g], e = p->g_order.begin() + bounds[g + 1];
+    std::iota(b, e, bounds[g]);
+    std::stable_sort(b, e, [&](int x, int y) { return p->n[x] > p->n[y]; });
+    int sp = bounds[g];
+    while (sp < bounds[g + 1] && p->n[p->g_order[sp]] > p->small_limit) ++sp;
+    p->g_split[g] = sp;
+  }
+  for (int i = 0; i < cnt; ++i) p->g_nb[i] = p->nb_bucket[bucket_of(p->n[p->g_order[i]])];
+  if (!p->d_gsys) {
+    RM_TRY(upload(&p->d_gsys, p->g_order));
+    RM_TRY(upload(&p->d_gnb, p->g_nb));
+  } else {
+    RM_CUDA_TRY(cudaMemcpy(p->d_gsys, p->g_order.data(), cnt * sizeof(int), cudaMemcpyHostToDevice));
+    RM_CUDA_TRY(cudaMemcpy(p->d_gnb, p->g_nb.data(), cnt * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  if (!p->copy_in) {
+    RM_CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_in, cudaStreamNonBlocking));
+    RM_CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_out, cudaStreamNonBlocking));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_start, cudaEventDisableTiming));
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_end, cudaEventDisableTiming));
+  }
+  while ((int)p->g_in.size() < G) {
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+    p->g_in.push_back(e1);
+    RM_CUDA_TRY(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+    p->g_done.push_back(e2);
+  }
+  p->groups_gen = p->tune_gen;
+  return RM_OK;
+}
+
+// The packed range [lo, hi) of items that the systems [s0, s1) use in an array with offsets off
+// and per-system sizes n * w (w = n for A, k for b and x).
+static void packed_range(const BatchPlan* p, const std::vector<int64_t>& off, bool square, int s0, int s1, int64_t& lo,
+                         int64_t& hi) {
+  lo = INT64_MAX, hi = 0;
+  for (int i = s0; i < s1; ++i) {
+    lo = std::min(lo, off[i]);
+    hi = std::max(hi, off[i] + (int64_t)p->n[i] * (square ? p->n[i] : p->k[i]));
+  }
+  if (lo > hi) lo = hi;
+}
+
+// Host A and b in, the solves, host x out: group by group, the copies of one group overlap the
+// solves of another (copy-in, solve and copy-out each on a stream of their own, ordered by
+// events). Ordered after prior work on s and before later work on s.
+int batch_plan_execute_host(BatchPlan* p, const double* h_a, const double* h_b, double* h_x, double* d_a, double* d_b,
+                            double* d_x, cudaStream_t s) {
+  if (!p) return RM_BAD_ARG;
+  if (p->count == 0) return RM_OK;
+  if (p->groups_gen != p->tune_gen) RM_TRY(build_groups(p));
+  const int G = (int)p->g_first.size() - 1;
+  RM_CUDA_TRY(cudaEventRecord(p->ev_start, s));
+  for (cudaStream_t q : {p->copy_in, p->stream, p->copy_out}) RM_CUDA_TRY(cudaStreamWaitEvent(q, p->ev_start, 0));
+  for (int g = 0; g < G; ++g) {
+    const int s0 = p->g_first[g], s1 = p->g_first[g + 1];  // systems (and items) of the group
+    int64_t lo, hi;
+    packed_range(p, p->a_off, true, s0, s1, lo, hi);
+    if (hi > lo) RM_CUDA_TRY(cudaMemcpyAsync(d_a + lo, h_a + lo, (hi - lo) * 8, cudaMemcpyHostToDevice, p->copy_in));
+    packed_range(p, p->b_off, false, s0, s1, lo, hi);
+    if (hi > lo) RM_CUDA_TRY(cudaMemcpyAsync(d_b + lo, h_b + lo, (hi - lo) * 8, cudaMemcpyHostToDevice, p->copy_in));
+    RM_CUDA_TRY(cudaEventRecord(p->g_in[g], p->copy_in));
+    RM_CUDA_TRY(cudaStreamWaitEvent(p->stream, p->g_in[g], 0));
+    auto args = [&](int f, int l, int* counter) {
+      BatchArgs q = batch_args(p, d_a, d_b, d_x, f, l, counter);
+      q.sys = p->d_gsys, q.nb = p->d_gnb;
+      return q;
+    };
+    RM_TRY(launch_split(
+        p, s0, s1, p->g_split[g], p->stream, true,
+        [&](int f, int l, cudaStream_t st) { bt::launch_solve(args(f, l, p->d_counter), std::min(p->grid, l - f), st); },
+        [&](int f, int l, cudaStream_t st) {
+          bt64::launch_solve(args(f, l, p->d_counter + 1), std::min(p->grid_small, l - f), st);
+        }));
+    RM_CUDA_TRY(cudaEventRecord(p->g_done[g], p->stream));
+    RM_CUDA_TRY(cudaStreamWaitEvent(p->copy_out, p->g_done[g], 0));
+    packed_range(p, p->x_off, false, s0, s1, lo, hi);
+    if (hi > lo) RM_CUDA_TRY(cudaMemcpyAsync(h_x + lo, d_x + lo, (hi - lo) * 8, cudaMemcpyDeviceToHost, p->copy_out));
+  }
+  RM_CUDA_TRY(cudaEventRecord(p->ev_end, p->copy_out));
+  RM_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_end, 0));
+  return RM_OK;
 }
 
 // dL/db = A^-T g and dL/dA = -(dL/db) x^T for every system, from the factors the last
@@ -368,7 +505,7 @@ int batch_plan_adjoint(BatchPlan* p, const double* a, const double* x, const dou
     return aj;
   };
   RM_TRY(launch_split(
-      p, 0, (int)p->count, p->stream, true,
+      p, 0, (int)p->count, p->split, p->stream, true,
       [&](int f, int l, cudaStream_t st) { bt::launch_adjoint(args(f, l, p->d_counter), std::min(p->grid, l - f), st); },
       [&](int f, int l, cudaStream_t st) {
         bt64::launch_adjoint(args(f, l, p->d_counter + 1), std::min(p->grid_small, l - f), st);
@@ -451,6 +588,12 @@ int rm_batch_plan_tune(rm_batch_plan* plan, const double* d_a, const double* d_b
 int rm_batch_plan_execute(rm_batch_plan* plan, const double* d_a, const double* d_b, double* d_x, void* stream) {
   if (!plan || (plan->p->count > 0 && (!d_a || !d_b || !d_x))) return RM_BAD_ARG;
   return rm::batch_plan_execute(plan->p, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rm_batch_plan_execute_host(rm_batch_plan* plan, const double* h_a, const double* h_b, double* h_x, double* d_a,
+                               double* d_b, double* d_x, void* stream) {
+  if (!plan || (plan->p->count > 0 && (!h_a || !h_b || !h_x || !d_a || !d_b || !d_x))) return RM_BAD_ARG;
+  return rm::batch_plan_execute_host(plan->p, h_a, h_b, h_x, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int rm_batch_plan_results(rm_batch_plan* plan, double* h_berr, int32_t* h_iters, int32_t* h_flags,

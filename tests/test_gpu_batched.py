@@ -186,3 +186,68 @@ def test_host_form(rb):
     _lib.check(st, "rm_dsolve_batched_host")
     Xs = [x[o:o + n * k].reshape(n, k) for o, n, k in zip(b_off, sizes, ks)]
     check_bar(As, Bs, Xs)
+
+
+def test_execute_from_host_memory(rb):
+    """execute_host (copies in groups that overlap the solves) gives the same bits as execute,
+    also after a tune (which may change the panel widths, so both run again), and with offsets
+    that do not follow the systems' order (one group)."""
+    import torch
+    rng = np.random.default_rng(11)
+    sizes = list(rng.integers(8, 257, 200)) + [3, 64, 65, 256]
+    ks = list(rng.integers(1, 5, len(sizes)))
+    As, Bs = batch(sizes, ks, shifted, seed=300)
+    plan = rb.BatchPlan(sizes, ks, method="mixed")
+    a, b = plan.pack(As, Bs, device="cuda")
+    x = torch.zeros(plan.b_size, dtype=torch.float64, device="cuda")
+    plan.execute(a, b, x)
+    torch.cuda.synchronize()
+    want = x.cpu()
+    a_h, b_h = a.cpu().pin_memory(), b.cpu().pin_memory()
+    x_h = torch.zeros(plan.b_size, dtype=torch.float64).pin_memory()
+    a2, b2, x2 = torch.zeros_like(a), torch.zeros_like(b), torch.zeros_like(x)
+    plan.execute_host(a_h, b_h, x_h, a2, b2, x2)
+    torch.cuda.synchronize()
+    assert torch.equal(x_h, want)
+    assert plan.results()[3].fell_back == 0
+    plan.tune(a, b, x)  # new panel widths (and so other float32 roundings): compare anew
+    plan.execute(a, b, x)
+    torch.cuda.synchronize()
+    want = x.cpu()
+    x_h.zero_()
+    plan.execute_host(a_h, b_h, x_h, a2, b2, x2)
+    torch.cuda.synchronize()
+    assert torch.equal(x_h, want)
+    check_bar(As, Bs, [t.numpy() for t in plan.unpack(x_h)])
+    plan.close()
+    # systems packed in reverse order: one group
+    from rustymath_b200 import _lib
+    import ctypes
+    ns = np.array([5, 40, 90], np.int64)
+    kk = np.array([1, 2, 3], np.int64)
+    a_off = np.array([40 * 40 + 90 * 90, 90 * 90, 0], np.int64)
+    b_off = np.array([2 * 40 + 3 * 90, 3 * 90, 0], np.int64)
+    As3, Bs3 = batch(list(ns), list(kk), shifted, seed=400)
+    a3 = np.zeros(int((ns * ns).sum()))
+    b3 = np.zeros(int((ns * kk).sum()))
+    for i in range(3):
+        a3[a_off[i]:a_off[i] + ns[i] ** 2] = As3[i].ravel()
+        b3[b_off[i]:b_off[i] + ns[i] * kk[i]] = Bs3[i].ravel()
+    h = ctypes.c_void_p()
+    lib = _lib.load()
+    _lib.check(lib.rm_batch_plan_create(3, ns.ctypes.data, kk.ctypes.data, a_off.ctypes.data, b_off.ctypes.data,
+                                        b_off.ctypes.data, None, ctypes.byref(h)), "plan")
+    ah, bh = torch.tensor(a3).pin_memory(), torch.tensor(b3).pin_memory()
+    xh = torch.zeros_like(bh).pin_memory()
+    ad, bd, xd = torch.zeros(a3.size, dtype=torch.float64, device="cuda"), torch.zeros(b3.size, dtype=torch.float64,
+                                                                                        device="cuda"), \
+        torch.zeros(b3.size, dtype=torch.float64, device="cuda")
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(lib.rm_batch_plan_execute_host(h, ctypes.c_void_p(ah.data_ptr()), ctypes.c_void_p(bh.data_ptr()),
+                                              ctypes.c_void_p(xh.data_ptr()), ctypes.c_void_p(ad.data_ptr()),
+                                              ctypes.c_void_p(bd.data_ptr()), ctypes.c_void_p(xd.data_ptr()), s), "ex")
+    torch.cuda.synchronize()
+    for i in range(3):
+        xi = xh.numpy()[b_off[i]:b_off[i] + ns[i] * kk[i]].reshape(ns[i], kk[i])
+        assert O.backward_error(As3[i], xi, Bs3[i]) <= ns[i] * 2.0 ** -53
+    lib.rm_batch_plan_destroy(h)
