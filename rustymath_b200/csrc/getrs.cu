@@ -747,31 +747,34 @@ int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, 
 // the diagonal blocks of pre are not written. With them a triangular solve is
 // x_b = D_b^-1 y_b - sum_j pre_bj x_j: every block's last step is a single product.
 // On the tensor cores, for 128-row blocks: out = D_b^-1 T_bj with
-// 3xTF32 mma.sync (float32-level products). 8 warps, warp w the rows 16w .. 16w+15 of all 16
-// column tiles; the operands in padded shared memory (A rows 132 floats apart, B rows 136:
-// both fragment patterns hit 32 distinct banks).
+// 3xTF32 mma.sync (float32-level products), a CTA per 64-column half of a block (104 KB of
+// shared memory: two CTAs per SM, so one CTA's loads overlap the other's products). 8 warps,
+// warp w the rows 16w .. 16w+15 of the 8 column tiles; the operands in padded shared memory (A
+// rows 132 floats apart, B rows 72: both fragment patterns hit 32 distinct banks).
 __global__ void __launch_bounds__(256) premultiply_mma_kernel(const float* __restrict__ w, int64_t ldw, int64_t n,
                                                               const float* __restrict__ dinv, float* __restrict__ pre,
                                                               int64_t ldp) {
-  constexpr int TB = 128, SA = 132, SB = 136;
+  constexpr int TB = 128, TN = 64, SA = 132, SB = 72;
   extern __shared__ uint8_t smraw[];
   float(*di)[SA] = reinterpret_cast<float(*)[SA]>(smraw);
   float(*ob)[SB] = reinterpret_cast<float(*)[SB]>(smraw + (size_t)TB * SA * sizeof(float));
   const int nblk = (int)((n + TB - 1) / TB);
-  const int b = blockIdx.x / nblk, j = blockIdx.x % nblk;
+  const int half = blockIdx.x & 1, blk = blockIdx.x >> 1;
+  const int b = blk / nblk, j = blk % nblk;
   if (b == j) return;
   const int which = j < b ? 0 : 1;
-  const int64_t r0 = (int64_t)b * TB, c0 = (int64_t)j * TB;
+  const int64_t r0 = (int64_t)b * TB, c0 = (int64_t)j * TB + half * TN;
   const float* dv = dinv + ((int64_t)b * kDiagMats + which) * TB * TB;
   {
-    // both operands as 16-byte loads, all 32 of a thread's in flight before any store
-    constexpr int PER = TB * TB / 4 / 256;  // float4 items per thread and operand
-    float4 va[PER], vb[PER];
+    // both operands as 16-byte loads, all 24 of a thread's in flight before any store
+    constexpr int PA = TB * TB / 4 / 256, PB = TB * TN / 4 / 256;  // float4 items per thread
+    float4 va[PA], vb[PB];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
+    for (int q = 0; q < PA; ++q) va[q] = __ldg(reinterpret_cast<const float4*>(dv + (threadIdx.x + q * 256) * 4));
+#pragma unroll
+    for (int q = 0; q < PB; ++q) {
       const int e = (threadIdx.x + q * 256) * 4;
-      const int i = e / TB, c = e % TB;
-      va[q] = __ldg(reinterpret_cast<const float4*>(dv + e));
+      const int i = e / TN, c = e % TN;
       const int64_t gi = r0 + i, gj = c0 + c;
       const float* src = w + gi * ldw + gj;
       if (gi < n && gj + 3 < n) {
@@ -784,29 +787,32 @@ __global__ void __launch_bounds__(256) premultiply_mma_kernel(const float* __res
       }
     }
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
+    for (int q = 0; q < PA; ++q) {
       const int e = (threadIdx.x + q * 256) * 4;
-      const int i = e / TB, c = e % TB;
-      *reinterpret_cast<float4*>(&di[i][c]) = va[q];
-      *reinterpret_cast<float4*>(&ob[i][c]) = vb[q];
+      *reinterpret_cast<float4*>(&di[e / TB][e % TB]) = va[q];
+    }
+#pragma unroll
+    for (int q = 0; q < PB; ++q) {
+      const int e = (threadIdx.x + q * 256) * 4;
+      *reinterpret_cast<float4*>(&ob[e / TN][e % TN]) = vb[q];
     }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
   const int ra = 16 * warp + g;
-  float d[16][4];
+  float d[TN / 8][4];
 #pragma unroll
-  for (int nt = 0; nt < 16; ++nt)
+  for (int nt = 0; nt < TN / 8; ++nt)
 #pragma unroll
     for (int e = 0; e < 4; ++e) d[nt][e] = 0.f;
   for (int k8 = 0; k8 < TB; k8 += 8) {
     const float a[4] = {di[ra][k8 + tq], di[ra + 8][k8 + tq], di[ra][k8 + tq + 4], di[ra + 8][k8 + tq + 4]};
 #pragma unroll
-    for (int nt = 0; nt < 16; ++nt) tc::mma_3xtf32(d[nt], a, ob[k8 + tq][8 * nt + g], ob[k8 + tq + 4][8 * nt + g]);
+    for (int nt = 0; nt < TN / 8; ++nt) tc::mma_3xtf32(d[nt], a, ob[k8 + tq][8 * nt + g], ob[k8 + tq + 4][8 * nt + g]);
   }
   float* out = pre + r0 * ldp + c0;
 #pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
+  for (int nt = 0; nt < TN / 8; ++nt) {
     const int col = 8 * nt + 2 * tq;
     *reinterpret_cast<float2*>(out + (int64_t)ra * ldp + col) = make_float2(d[nt][0], d[nt][1]);
     *reinterpret_cast<float2*>(out + (int64_t)(ra + 8) * ldp + col) = make_float2(d[nt][2], d[nt][3]);
@@ -822,9 +828,9 @@ size_t premultiplied_f32_bytes(int64_t n) {
 int premultiply_f32(const float* lu, int64_t ld, int64_t n, const float* dinv, float* pre, cudaStream_t stream) {
   const int nblk = (int)((n + kTB32 - 1) / kTB32);
   if (nblk < 2) return RM_OK;
-  const size_t smem = (size_t)kTB32 * (132 + 136) * sizeof(float);
+  const size_t smem = (size_t)kTB32 * (132 + 72) * sizeof(float);
   RM_TRY(smem_attribute(premultiply_mma_kernel, smem));
-  premultiply_mma_kernel<<<nblk * nblk, 256, smem, stream>>>(lu, ld, n, dinv, pre, premultiplied_f32_ld(n));
+  premultiply_mma_kernel<<<2 * nblk * nblk, 256, smem, stream>>>(lu, ld, n, dinv, pre, premultiplied_f32_ld(n));
   RM_LAUNCHED();
   return RM_OK;
 }
