@@ -771,13 +771,14 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
     PhaseTrace tr(s, "mixed float32 + float64 refinement solve");
     RM_TRY(to_f32(d_a, n, n, f, ldf, s));
     tr.mark("to_f32");
-    // long chains (n > 1024) solve on block-Jacobi-scaled triangles, whose diagonal inverses the
-    // panels write as they go; shorter ones invert the diagonal blocks and their couplings here
+    // the panels write their diagonal blocks' inverses into the solves' table as they go; long
+    // chains (n > 1024) then solve on block-Jacobi-scaled triangles, shorter ones take the
+    // blocks' couplings to their predecessors
     float* pre = n > 1024 ? sc.at<float>(opre) : nullptr;  // worth its one-off cost on long chains
-    RM_TRY(getrf_lpp_f32(f, ldf, n, perm, sc.at<void>(olu), st, s, pre ? sc.at<float>(odinv) : nullptr));
+    RM_TRY(getrf_lpp_f32(f, ldf, n, perm, sc.at<void>(olu), st, s, sc.at<float>(odinv)));
     tr.mark("getrf_f32");
     if (pre) RM_TRY(premultiply_f32(f, ldf, n, sc.at<float>(odinv), pre, s));
-    else RM_TRY(invert_diag_blocks_f32(f, ldf, n, sc.at<float>(odinv), s));
+    else RM_TRY(couplings_f32(f, ldf, n, sc.at<float>(odinv), s));
     tr.mark("solve_setup");
     // x0 = (LU)^-1 P b
     RM_TRY(gather_f32(d_b, k, perm, n, k, c, k, s));

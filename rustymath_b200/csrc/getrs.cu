@@ -742,6 +742,16 @@ int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, 
   return launch_invert<float, false, kTB32>(w, ldw, n, dinv, true, false, stream);
 }
 
+int couplings_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream) {
+  const int nblk = (int)((n + kTB32 - 1) / kTB32);
+  if (nblk < 2) return RM_OK;
+  const size_t smem = (size_t)kTB32 * (kTB32 + 1) * sizeof(float);
+  RM_TRY(smem_attribute(coupling_kernel<float, false, kTB32>, 2 * smem));
+  coupling_kernel<float, false, kTB32><<<dim3((unsigned)nblk, 2), 256, 2 * smem, stream>>>(w, ldw, n, dinv);
+  RM_LAUNCHED();
+  return RM_OK;
+}
+
 // pre = the block-Jacobi-scaled triangles of the row-major float32 L\U w: block (b, j) of pre is
 // dinv[b][0] L_bj below the diagonal blocks (j < b) and dinv[b][1] U_bj above them (j > b);
 // the diagonal blocks of pre are not written. With them a triangular solve is

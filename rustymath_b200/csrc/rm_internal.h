@@ -156,6 +156,9 @@ int accumulate_f64(const float* c, int64_t ldc, int64_t n, int64_t k, double* x,
 // float32 triangular solves of an unpivoted row-major L\U (getrs.cu)
 size_t diag_blocks_f32_bytes(int64_t n);
 int invert_diag_blocks_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream);
+// Entries [2] and [3] of the float32 table (the couplings to the block before), from entries [0]
+// and [1], which the factorization's panels wrote
+int couplings_f32(const float* w, int64_t ldw, int64_t n, float* dinv, cudaStream_t stream);
 size_t trsv_f32_scratch_bytes(int64_t n, int64_t k);
 int64_t premultiplied_f32_ld(int64_t n);
 size_t premultiplied_f32_bytes(int64_t n);
