@@ -41,6 +41,38 @@ def _jsonable(o):
     return str(o)
 
 
+_collect = False  # set while the headline run gathers the other configurations' lines
+
+
+def _emit(line):
+    """Prints a workload's JSON line, or hands it back while the headline run collects them."""
+    if not _collect:
+        print(json.dumps(line, default=_jsonable), flush=True)
+    return line
+
+
+def other_configs(args, local):
+    """The other configurations, measured in the same run on one GPU (each its own timed region,
+    after the headline's): n = 512 (plain and mixed solves, 512^3 product), the 20,000 uneven
+    systems, the 4096-system adjoint and the 16384^3 GEMM. A leg that fails reports its error."""
+    global _collect
+    out = {}
+    _collect = True
+    try:
+        for name, fn in (("c1_n512", run_small), ("c3_batched_20000", run_batched),
+                         ("c4_adjoint_4096x64", run_adjoint), ("c5_gemm_16384", run_gemm)):
+            t0 = time.perf_counter()
+            try:
+                sub = fn(args, 0, 1, local)
+                sub["wall_s"] = time.perf_counter() - t0
+                out[name] = sub
+            except Exception as e:  # noqa: BLE001 - reported in the line, the headline stands
+                out[name] = {"error": f"{type(e).__name__}: {e}"}
+    finally:
+        _collect = False
+    return out
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -51,6 +83,8 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--method", default="auto", choices=["auto", "plain", "mixed"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-other-configs", action="store_true",
+                   help="headline only: skip the other configurations' legs of the default run")
     p.add_argument("--solve-only", action="store_true",
                    help="only the timed solves (for profiling): no e2e, roofline or CPU legs")
     p.add_argument("--workload", default="single", choices=["single", "batched", "adjoint", "gemm", "update", "small"],
@@ -440,7 +474,7 @@ def run_batched(args, rank, world, local):
         line["parity_vs_oracle"] = batch_parity(ns, ks, a_h.numpy(), b_h.numpy(),
                                                 {"plain_fp64": x_plain.cpu().numpy(), "mixed": x_mixed.cpu().numpy()},
                                                 sample=500)
-    print(json.dumps(line, default=_jsonable), flush=True)
+    return _emit(line)
 
 
 def batch_parity(ns, ks, a_h, b_h, arms, sample, seed=0):
@@ -469,7 +503,10 @@ def batch_parity(ns, ks, a_h, b_h, arms, sample, seed=0):
             res[name] = (fwd, fwd / bound)
         return res
 
-    with ThreadPoolExecutor(os.cpu_count()) as ex:
+    # one BLAS thread per worker: NumPy's LAPACK calls (cond) from many threads at once, each
+    # multithreaded, oversubscribe the cores (200x slower)
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(1), ThreadPoolExecutor(os.cpu_count()) as ex:
         rows = list(ex.map(one, idx))
     out = {"systems_checked": len(idx), "sample": f"{len(idx)} systems drawn by default_rng({seed})"}
     for name in arms:
@@ -574,7 +611,7 @@ def run_adjoint(args, rank, world, local):
                                            "full size (profiles/batch_kernels_n64x4096.md)",
                          "note": "algorithmic bytes: A read once (transposed residual) + dA written once"},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary()}
-    print(json.dumps(line, default=_jsonable), flush=True)
+    return _emit(line)
 
 
 GEMM_METRIC = "FP64-accurate GEMM TFLOP/s at 16384^3: Ozaki int8 split vs native FP64 on one B200"
@@ -652,7 +689,7 @@ def run_gemm(args, rank, world, local):
             "cublas_fp64": {"tflops": fl / t_cub / 1e12, "ms": 1e3 * t_cub},
             "cross_check_2048_vs_oracle": cross, "gemv": gemv,
             "gpu_launches": int(launches), "clocks": clocks.summary()}
-    print(json.dumps(line, default=_jsonable), flush=True)
+    return _emit(line)
 
 
 def gemv_legs(torch, lib, a, dev, steps):
@@ -788,7 +825,7 @@ def run_small(args, rank, world, local):
             "gpu": out, "cpu_baseline": {"kind": "port", "cores": os.cpu_count(), **cpu},
             "gflops": {"solve_plain": (2 / 3 * n ** 3 + 2 * n * n) / out["solve_plain_ms"] / 1e6,
                        "matmul": 2 * n ** 3 / out["matmul_ms"] / 1e6}}
-    print(json.dumps(line, default=_jsonable), flush=True)
+    return _emit(line)
 
 
 def run_update(args, rank, world, local):
@@ -955,6 +992,8 @@ def main():
                 "plain_vs_cusolver_time_ratio": plain["ms_per_solve"] / cusolver["ms_per_solve"],
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks.summary(), "tflops_lu": (2.0 / 3.0) * n ** 3 / (elapsed / args.steps) / 1e12 * world}
+        if world == 1 and not args.no_other_configs:
+            line["other_configs"] = other_configs(args, local)
         print(json.dumps(line, default=_jsonable), flush=True)
     if world > 1:
         dist.barrier()

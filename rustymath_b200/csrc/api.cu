@@ -81,12 +81,8 @@ unsigned* device_status() {
   return ptrs[dev];
 }
 
-int take_device_status(cudaStream_t stream) {
-  unsigned* st = device_status();
-  if (!st) return RM_CUDA_ERROR;
-  unsigned h = 0;
-  RM_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream));
-  RM_CUDA_TRY(cudaStreamSynchronize(stream));
+// Maps a status word read back from the device to a status code and clears the word.
+static int status_from_word(unsigned h, unsigned* st, cudaStream_t stream) {
   if (h) {
     RM_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(unsigned), stream));
     if (h & RM_DEV_TIMEOUT) {
@@ -99,6 +95,53 @@ int take_device_status(cudaStream_t stream) {
     }
   }
   return RM_OK;
+}
+
+int take_device_status(cudaStream_t stream) {
+  unsigned* st = device_status();
+  if (!st) return RM_CUDA_ERROR;
+  unsigned h = 0;
+  RM_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream));
+  RM_CUDA_TRY(cudaStreamSynchronize(stream));
+  return status_from_word(h, st, stream);
+}
+
+// What a synchronous call reads back at its end, in page-locked memory so that the copies stay
+// asynchronous and the host waits once. One block per host thread, allocated at its first use
+// and kept until the process exits.
+struct alignas(16) CallResults {
+  unsigned status;
+  int32_t flag;
+  double berr[2];
+};
+
+static CallResults* call_results() {
+  static thread_local CallResults* p = nullptr;
+  if (!p && cudaHostAlloc(reinterpret_cast<void**>(&p), sizeof(CallResults), cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+  }
+  return p;
+}
+
+// Ends a synchronous call with one wait: the device status word, and the int32 flag and two
+// doubles at d_flag / d_berr when given, read back together. The status word's errors come first.
+static int finish_call(cudaStream_t s, const int32_t* d_flag, int32_t* flag, const double* d_berr, double* berr) {
+  unsigned* st = device_status();
+  if (!st) return RM_CUDA_ERROR;
+  CallResults* h = call_results();
+  if (!h) {  // no page-locked block: one pageable read each
+    if (d_flag) RM_CUDA_TRY(cudaMemcpyAsync(flag, d_flag, sizeof *flag, cudaMemcpyDeviceToHost, s));
+    if (d_berr) RM_CUDA_TRY(cudaMemcpyAsync(berr, d_berr, 2 * sizeof *berr, cudaMemcpyDeviceToHost, s));
+    return take_device_status(s);
+  }
+  RM_CUDA_TRY(cudaMemcpyAsync(&h->status, st, sizeof h->status, cudaMemcpyDeviceToHost, s));
+  if (d_flag) RM_CUDA_TRY(cudaMemcpyAsync(&h->flag, d_flag, sizeof h->flag, cudaMemcpyDeviceToHost, s));
+  if (d_berr) RM_CUDA_TRY(cudaMemcpyAsync(h->berr, d_berr, sizeof h->berr, cudaMemcpyDeviceToHost, s));
+  RM_CUDA_TRY(cudaStreamSynchronize(s));
+  if (d_flag) *flag = h->flag;
+  if (d_berr) berr[0] = h->berr[0], berr[1] = h->berr[1];
+  return status_from_word(h->status, st, s);
 }
 
 // ------------------------------------------------------------------ failure injection (tests)
@@ -714,33 +757,35 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   RM_TRY(getrf_f64(w, lb.ldw, n, sc.at<int64_t>(lb.ipiv), sc.at<int64_t>(lb.perm), sc.at<void>(lb.getrf),
                    device_status(), s));
   tr.mark("getrf");
+  // The regular flag, the backward error and the device status word are read back together at
+  // the end: the host waits once per call. A matrix that is not regular still gets
+  // RM_NOT_REGULAR; x is then unspecified.
   RM_TRY(regular_flag_f64(w, lb.ldw, n, sc.at<double>(lb.amax), sc.at<int32_t>(lb.flag), s));
-  int32_t regular = 0;
-  RM_CUDA_TRY(cudaMemcpyAsync(&regular, sc.at<int32_t>(lb.flag), sizeof regular, cudaMemcpyDeviceToHost, s));
-  RM_TRY(take_device_status(s));
-  if (report) report->regular = regular;
-  if (!regular) {
-    set_last_message("a pivot is at most eps*n*max|a|; rustymath's solve takes least squares here");
-    return RM_NOT_REGULAR;
-  }
   RM_TRY(invert_diag_blocks_f64(w, lb.ldw, false, n, sc.at<double>(lb.dinv), true, false, s));
   tr.mark("regular");
   RM_TRY(getrs_f64(w, lb.ldw, false, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k,
                    sc.at<void>(os), device_status(), s));
   tr.mark("getrs");
   if (report) {
-    double berr[2] = {0, 0};
     RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
     RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(lb.berr), s));
     tr.mark("residual");
-    RM_CUDA_TRY(cudaMemcpyAsync(berr, sc.at<double>(lb.berr), sizeof berr, cudaMemcpyDeviceToHost, s));
-    RM_TRY(take_device_status(s));
+  }
+  int32_t regular = 0;
+  double berr[2] = {0, 0};
+  RM_TRY(finish_call(s, sc.at<int32_t>(lb.flag), &regular, report ? sc.at<double>(lb.berr) : nullptr, berr));
+  if (report) report->regular = regular;
+  if (!regular) {
+    set_last_message("a pivot is at most eps*n*max|a|; rustymath's solve takes least squares here");
+    return RM_NOT_REGULAR;
+  }
+  if (report) {
     report->backward_error = berr[0];
     report->iterations = 0;
     report->method_used = RM_METHOD_PLAIN_F64;
     report->fell_back = 0;
   }
-  return take_device_status(s);
+  return RM_OK;
 }
 
 // The mixed-precision solve: float32 LU on the tensor cores (panels pivoted among their own

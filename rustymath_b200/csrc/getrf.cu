@@ -449,6 +449,187 @@ __global__ void __launch_bounds__(kShortLeafMaxRows, 1)
     if (lane < jb) w[(int64_t)(j0 + sh.pos[r2]) * ldw + j0 + lane] = S[r2 * kShortStride + lane];
 }
 
+// ------------------------------------------------------------------ a whole matrix in a cluster
+// n <= 256: the whole matrix lives in the shared memory of one cluster of C <= 8 CTAs (a power
+// of two, at most 32 rows per CTA; 66 KB per CTA at n = 256) and is factored in one launch,
+// column by column, right-looking, with one cluster barrier per pivot column, in place of the
+// blocked path's chain of dependent launches (leaves, swaps, inversions, block products). Each
+// item takes the fmas of rustymath's packed products in the same order (one per pivot column,
+// in column order), so the factors are the oracle's bits. Measured per solve (n = 128 / 192 /
+// 256): 0.29 / 0.41 / 0.51 ms against 0.31 / 0.47 / 0.57 ms on the blocked path; a column costs
+// ~1.1 us at C = 2 and ~2.2 us at C = 16 (the cluster barrier and the pivot row's reads from one
+// CTA's shared memory), so at n = 384..512 the blocked path is faster and keeps those sizes.
+//
+// Rows do not move. Every warp of a CTA tracks the positions of the CTA's rows (lane = row), so
+// a pivot choice only exchanges two positions, as in short_leaf_kernel; at the end each row is
+// stored at its final position. Per pivot column j, after the barrier that publishes column j's
+// candidates:
+//   - every warp reduces the C posts (largest key, lowest position among equals; when every
+//     candidate is NaN, the row at position j, which its CTA posts beside its candidate) and
+//     forms its rows' multipliers l = a_ij / pivot (the reciprocal as the other panels form it);
+//   - warp 0 updates column j + 1 (the pivot row's item read from the winner's shared memory),
+//     keeps it, finds its CTA's candidate for column j + 1 and posts it into every CTA's slot;
+//   - the other warps update columns j + 2 .. n - 1, 32 columns per warp, the pivot row's items
+//     read from the winner's shared memory a lane each and passed on by shuffles.
+// Posts are double-buffered by the column's parity: a CTA writes the slot of column j + 2 only
+// after the barrier of column j + 1, which every CTA reaches after it has read column j's posts.
+// Each item takes one fma per pivot column, in column order; a zero pivot leaves its column
+// unreduced (factor.rs:606); the multipliers of column j are written into column j at the next
+// step, when no warp reads that column any more. Every CTA runs the same n barriers, so the
+// barrier cannot be left waiting.
+constexpr int kClusterLuMax = 256;
+constexpr int kClusterLuRows = 32;  // rows per CTA at most (a lane each)
+
+struct alignas(16) ClusterPost {
+  unsigned long long key;  // |candidate| bits + 1; 0 for NaN or no row left
+  double piv;              // the candidate's item
+  double dpiv;             // the item of the row at the diagonal's position, when this CTA holds it
+  int pos;                 // the candidate's position
+  int lrow;                // its row within the CTA
+  int drow;                // the CTA's row at the diagonal's position, or -1
+  int pad;
+};
+
+struct ClusterLuShared {
+  ClusterPost post[2][kMaxCluster];  // [column parity][posting CTA]
+};
+
+__device__ __forceinline__ void st_cluster_u64(uint32_t a, unsigned long long v) {
+  asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory");
+}
+
+// Warp 0 of each CTA: the CTA's candidate for column `col` (y = this lane's row's item) and, if
+// the CTA holds it, the row at position `col`, stored into slot `slot` of every CTA's posts.
+__device__ __forceinline__ void cluster_lu_post(ClusterLuShared& sh, int slot, double y, int pos, bool active,
+                                                int col, int C, int rank, int lane) {
+  const double a = fabs(y);
+  const unsigned long long key = (active && a == a) ? (unsigned long long)__double_as_longlong(a) + 1ull : 0ull;
+  bool none;
+  const int wl = short_reduce(key, (unsigned)pos, none);
+  const unsigned long long wkey = __shfl_sync(0xffffffffu, key, wl);
+  const double wpiv = __shfl_sync(0xffffffffu, y, wl);
+  const int wpos = __shfl_sync(0xffffffffu, pos, wl);
+  const unsigned db = __ballot_sync(0xffffffffu, pos == col);
+  const int dl = db ? __ffs(db) - 1 : -1;
+  const double dpiv = __shfl_sync(0xffffffffu, y, dl < 0 ? 0 : dl);
+  if (lane < C) {
+    const uint32_t d = map_rank(&sh.post[slot][rank], (uint32_t)lane);
+    st_cluster_u64(d + offsetof(ClusterPost, key), wkey);
+    st_cluster(d + offsetof(ClusterPost, piv), wpiv);
+    st_cluster(d + offsetof(ClusterPost, dpiv), dpiv);
+    st_cluster(d + offsetof(ClusterPost, pos), wpos);
+    st_cluster(d + offsetof(ClusterPost, lrow), wl);
+    st_cluster(d + offsetof(ClusterPost, drow), dl);
+  }
+}
+
+// W (row-major, ldw) is factored in place: on return row i of W holds row i of the factors (the
+// source row perm[i]); ipiv[j] is the position exchanged with j at step j. R rows per CTA, ld
+// the shared row stride (odd: a warp's column reads hit distinct banks).
+__global__ void __launch_bounds__(32 * (1 + kClusterLuMax / 32), 1)
+    cluster_lu_kernel(double* __restrict__ w, int64_t ldw, int n, int R, int ld, int64_t* __restrict__ ipiv,
+                      int64_t* __restrict__ perm) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  ClusterLuShared& sh = *reinterpret_cast<ClusterLuShared*>(smem);
+  double* S = reinterpret_cast<double*>(smem + sizeof(ClusterLuShared));
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int rank = (int)cluster_ctarank(), C = (int)cluster_nctarank();
+  const int g0 = rank * R;
+  const int rows = max(0, min(R, n - g0));
+  for (int i = warp; i < rows; i += nwarps)
+    for (int c = lane; c < n; c += 32) S[i * ld + c] = w[(int64_t)(g0 + i) * ldw + c];
+  const bool valid = lane < rows;
+  int pos = valid ? g0 + lane : INT_MAX;
+  double* myrow = S + (valid ? lane : 0) * ld;
+  cluster_sync_all();  // the rows are in, and every CTA of the cluster runs before any DSMEM access
+  if (warp == 0) cluster_lu_post(sh, 0, valid ? myrow[0] : 0.0, pos, valid, 0, C, rank, lane);
+  cluster_sync_all();
+  double lprev = 0.0;  // warp 0: the multiplier of the step before, written one step late
+  bool lprev_set = false;
+#pragma unroll 1
+  for (int j = 0; j < n; ++j) {
+    const ClusterPost* pp = sh.post[j & 1];
+    const unsigned long long k2 = lane < C ? pp[lane].key : 0ull;
+    const unsigned p2 = lane < C ? (unsigned)pp[lane].pos : 0xffffffffu;
+    bool none;
+    int wr = short_reduce(k2, p2, none);
+    int lr, pr;
+    double piv;
+    if (!none) {
+      lr = pp[wr].lrow;
+      pr = pp[wr].pos;
+      piv = pp[wr].piv;
+    } else {  // every candidate is NaN: the row at position j is the pivot row
+      const unsigned b = __ballot_sync(0xffffffffu, lane < C && pp[lane].drow >= 0);
+      wr = __ffs(b) - 1;
+      lr = pp[wr].drow;
+      pr = j;
+      piv = pp[wr].dpiv;
+    }
+    if (pos == pr) pos = j;
+    else if (pos == j) pos = pr;
+    const bool active = valid && pos > j;
+    const bool skip = piv == 0.0;
+    const bool sub = fabs(piv) < 2.2250738585072014e-308;
+    const double rcp = short_rcp(piv);
+    double l = 0.0;
+    if (active && !skip) {
+      const double a = myrow[j];
+      l = sub ? a / piv : a * rcp;
+    }
+    const uint32_t prow = map_rank(S + lr * ld, (uint32_t)wr);  // the pivot row, in CTA wr
+    if (warp == 0) {
+      if (lprev_set) myrow[j - 1] = lprev;
+      lprev = l;
+      lprev_set = active && !skip;
+      if (j + 1 < n) {
+        double y = valid ? myrow[j + 1] : 0.0;
+        if (!skip) {
+          const double u = ld_cluster_f64(prow + (uint32_t)(j + 1) * 8u);
+          if (active) {
+            y = fma(l, -u, y);
+            myrow[j + 1] = y;
+          }
+        }
+        cluster_lu_post(sh, (j + 1) & 1, y, pos, active, j + 1, C, rank, lane);
+      }
+    } else if (!skip) {
+#pragma unroll 1
+      for (int c0 = j + 2 + (warp - 1) * 32; c0 < n; c0 += (nwarps - 1) * 32) {
+        const int cc = c0 + lane;
+        const double ul = cc < n ? ld_cluster_f64(prow + (uint32_t)cc * 8u) : 0.0;
+        const int cend = min(32, n - c0);
+        double* rp = myrow + c0;
+        if (cend == 32) {
+#pragma unroll 8
+          for (int q = 0; q < 32; ++q) {
+            const double u = __shfl_sync(0xffffffffu, ul, q);
+            if (active) rp[q] = fma(l, -u, rp[q]);
+          }
+        } else {
+          for (int q = 0; q < cend; ++q) {
+            const double u = __shfl_sync(0xffffffffu, ul, q);
+            if (active) rp[q] = fma(l, -u, rp[q]);
+          }
+        }
+      }
+    }
+    if (rank == 0 && t == 0) ipiv[j] = pr;
+    cluster_sync_all();
+  }
+  // every row to its final position: a warp per row, lanes along it
+  for (int i = warp; i < rows; i += nwarps) {
+    const int pi = __shfl_sync(0xffffffffu, pos, i);
+    for (int c = lane; c < n; c += 32) w[(int64_t)pi * ldw + c] = S[i * ld + c];
+  }
+  if (warp == 0 && valid) perm[pos] = g0 + lane;
+}
+
+constexpr size_t cluster_lu_smem(int R, int ld) {
+  return sizeof(ClusterLuShared) + (size_t)R * ld * sizeof(double);
+}
+
 // ------------------------------------------------------------------ swaps + unit-lower solve
 constexpr int kSwapCols = 16;      // columns per CTA
 constexpr int kSwapThreads = 256;
@@ -620,6 +801,72 @@ static int panel_cluster_limit() {
 }
 
 
+// Whether this device can place the largest cluster cluster_lu_kernel takes (8 CTAs of 288
+// threads and 66 KB of shared memory); found once per device.
+constexpr int kClusterLuMaxCtas = kClusterLuMax / kClusterLuRows;
+static bool find_cluster_lu_ok() {
+  const size_t smem = cluster_lu_smem(kClusterLuRows, kClusterLuMax + 1);
+  if (smem_attribute(cluster_lu_kernel, smem) != RM_OK) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kClusterLuMaxCtas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(kClusterLuMaxCtas);
+  cfg.blockDim = dim3(32 * (1 + kClusterLuMax / 32));
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, cluster_lu_kernel, &cfg) == cudaSuccess && clusters > 0) return true;
+  cudaGetLastError();
+  return false;
+}
+
+static bool cluster_lu_ok() {
+  static std::mutex mu;
+  static std::vector<int> state;  // 0 unknown, 1 yes, 2 no
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)state.size() > dev && state[dev]) return state[dev] == 1;
+  }
+  const bool ok = find_cluster_lu_ok();
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)state.size() <= dev) state.resize(dev + 1, 0);
+  state[dev] = ok ? 1 : 2;
+  return ok;
+}
+
+// n <= kClusterLuMax in one launch: C CTAs (the least power of two giving at most 32 rows each).
+static int launch_cluster_lu(double* w, int64_t ldw, int n, int64_t* ipiv, int64_t* perm, cudaStream_t stream) {
+  const int need = (n + kClusterLuRows - 1) / kClusterLuRows;
+  int C = 1;
+  while (C < need) C *= 2;
+  const int R = (n + C - 1) / C;
+  const int ld = n | 1;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(32 * (1 + (n + 31) / 32));
+  cfg.dynamicSmemBytes = cluster_lu_smem(R, ld);
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  RM_CUDA_TRY(cudaLaunchKernelEx(&cfg, cluster_lu_kernel, w, ldw, n, R, ld, ipiv, perm));
+  note_launch();
+  return RM_OK;
+}
+
 template <typename T>
 static int launch_panel(T* w, int64_t ldw, int n, int j0, int jb, int64_t* ipiv, cudaStream_t stream) {
   const int M = n - j0;
@@ -782,6 +1029,7 @@ int getrf_f64(double* w, int64_t ldw, int64_t n64, int64_t* ipiv, int64_t* perm,
   if (n64 <= 0) return RM_OK;
   if (n64 > INT32_MAX / 2) return RM_BAD_ARG;
   const int n = (int)n64;
+  if (n <= kClusterLuMax && cluster_lu_ok()) return launch_cluster_lu(w, ldw, n, ipiv, perm, caller);
   double* linv = reinterpret_cast<double*>(scratch);
   iota_kernel<<<std::max(1, std::min(n / 256 + 1, 1024)), 256, 0, caller>>>(perm, n);
   RM_LAUNCHED();

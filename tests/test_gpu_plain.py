@@ -94,6 +94,20 @@ def test_lu_matches_oracle(rb, n):
     assert distance(product(lower_of(f), upper_of(f)), a[p], max(norm(a), 1.0)) < 4 * EPS * max(n, 1)
 
 
+@pytest.mark.parametrize("n", [1, 2, 5, 31, 32, 33, 64, 71, 100, 128, 129, 200, 255, 256])
+def test_small_lu_is_the_oracles_bits(rb, n):
+    """Up to n = 256 the factorization is one cluster launch in which every item takes one fma
+    per pivot column in column order, which is how rustymath's lu_factor reaches it through
+    its packed products' in-order folds (core/src/linalg/factor.rs:580-630,
+    core/src/linalg.rs:1282): factors and positions are the oracle's, bit for bit, on the
+    reference tests' inputs and on N(0,1) matrices."""
+    for a in (ref_random(n, n, n + 1), np.random.default_rng(n).standard_normal((n, n))):
+        f, p = rb.lu(a)
+        fo, po = O.lu_factor(a)
+        assert np.array_equal(p, po)
+        assert np.array_equal(f, fo)
+
+
 @pytest.mark.parametrize("n", [1, 5, 33, 71, 530])
 def test_lu_solve_residuals(rb, n):
     """tests/linalg.rs:384-390: solve and inverse residuals below 4*eps*n."""
