@@ -835,8 +835,9 @@ static int dsolve_mixed(int64_t n, const double* d_a, const double* d_b, int64_t
       RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));
       RM_TRY(backward_error_f64(d_x, k, n, k, sc.at<double>(onorm), sc.at<double>(oberr), s));
       tr.mark("residual");
-      RM_CUDA_TRY(cudaMemcpyAsync(&berr_h, sc.at<double>(oberr), sizeof berr_h, cudaMemcpyDeviceToHost, s));
-      const int dst = take_device_status(s);  // synchronises
+      double be[2] = {0.0, 0.0};
+      const int dst = finish_call(s, nullptr, nullptr, sc.at<double>(oberr), be);  // synchronises once
+      berr_h = be[0];
       if (dst != RM_OK && dst != RM_TIMEOUT) return dst;
       if (dst == RM_TIMEOUT) {
         timed_out = true;
