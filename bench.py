@@ -405,9 +405,9 @@ def run_batched(args, rank, world, local):
     ns, ks, a, b = make_batch(args.count, 1 + rank, dev, args.uniform_n)
     x = torch.zeros(int((ns * ks).sum()), dtype=torch.float64, device=dev)
 
-    def arm(method, steps, clocks=None):
+    def arm(method, steps, clocks=None, precision=False):
         plan = rb.BatchPlan(ns, ks, method=method)
-        widths = plan.tune(a, b, x)
+        widths = plan.tune(a, b, x, precision=precision)
         for _ in range(max(args.warmup, 1)):
             plan.execute(a, b, x)
         torch.cuda.synchronize()
@@ -428,6 +428,15 @@ def run_batched(args, rank, world, local):
     clocks = ClockSampler(local)
     plan, t, rep, widths, launches = arm("mixed", args.steps, clocks)
     x_mixed = x.clone()
+    # the tuner's precision axis: per size bucket, float32 factors + refinement or float64 factors
+    plan_p, t_p, rep_p, _, _ = arm("mixed", max(1, min(args.steps, 3)), precision=True)
+    tuned = {"solves_per_s": len(ns) / t_p, "ms_per_step": 1e3 * t_p, "backward_error_max": rep_p.max_backward_error,
+             "route_by_bucket": plan_p.precision(), "buckets": "n <= 32, 64, 128, 192, 256",
+             "note": "BatchPlan(method='mixed').tune(precision=True): each bucket keeps the faster of float32 "
+                     "factors + float64 refinement and float64 factors; every system still <= n 2^-53"}
+    del plan_p
+    plan.execute(a, b, x)  # x holds the mixed arm's answer again for the copies and checks below
+    torch.cuda.synchronize()
     count = len(ns)
     # end to end: pinned host A, B -> device, the launch, X -> host, every step
     a_h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
@@ -457,6 +466,7 @@ def run_batched(args, rank, world, local):
             "max_iterations": rep.max_iterations,
             "plain_fp64": {"solves_per_s": count / t_plain, "ms_per_step": 1e3 * t_plain,
                            "backward_error_max": rep_plain.max_backward_error},
+            "tuned_precision": tuned,
             "roofline": {"bound": "hbm", "kernel": "batch_solve_kernel (whole batch; the n <= 64 systems on a "
                                                  "second launch beside it when the tuner keeps them there)",
                          "achieved": passes * a_bytes / t / 1e9, "peak": peak_hbm(), "unit": "GB/s",

@@ -282,6 +282,12 @@ int rm_batch_plan_create(int64_t count, const int64_t *h_n, const int64_t *h_k, 
  * fastest, then the CTA size (64 or 256 threads) for the systems of n <= 32 and n <= 64;
  * synchronises on `stream`. */
 int rm_batch_plan_tune(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x, void *stream);
+/* rm_batch_plan_tune with a precision axis as well (a plan made with RM_METHOD_F32_IR): each
+ * size bucket also times float64 factors without refinement and keeps whichever route is
+ * fastest, so every system still meets the plan's tolerance. rustymath's Stacked::solve has no
+ * tuner (every stack is float64); this chooses per size bucket. Synchronises on `stream`. */
+int rm_batch_plan_tune_precision(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x,
+                                 void *stream);
 /* One persistent kernel launch for all systems, replayed from a CUDA graph; asynchronous on
  * `stream`. */
 int rm_batch_plan_execute(rm_batch_plan *plan, const double *d_a, const double *d_b, double *d_x, void *stream);
@@ -314,6 +320,9 @@ int rm_batch_plan_panel_width(const rm_batch_plan *plan, int bucket);
 /* The threads per CTA (a thread per row) that solve size bucket 0..4: 64 or 256 (the
  * 64-thread build takes systems of n <= 64 unless the tuner chose otherwise). */
 int rm_batch_plan_cta_threads(const rm_batch_plan *plan, int bucket);
+/* The route size bucket 0..4 takes: RM_METHOD_F32_IR (float32 factors + float64 refinement) or
+ * RM_METHOD_PLAIN_F64 (float64 factors); -1 for a bad argument. */
+int rm_batch_plan_precision(const rm_batch_plan *plan, int bucket);
 int rm_batch_plan_destroy(rm_batch_plan *plan);
 /* create + execute + results + destroy; synchronises. RM_NO_CONVERGENCE when a system stalled
  * with fallback off. */

@@ -63,10 +63,12 @@ SIGNATURES = {
     "rm_batch_plan_create": (ctypes.c_int, [_i64, _p, _p, _p, _p, _p, ctypes.POINTER(SolveOptions),
                                             ctypes.POINTER(_p)]),
     "rm_batch_plan_tune": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "rm_batch_plan_tune_precision": (ctypes.c_int, [_p, _p, _p, _p, _p]),
     "rm_batch_plan_execute": (ctypes.c_int, [_p, _p, _p, _p, _p]),
     "rm_batch_plan_results": (ctypes.c_int, [_p, _p, _p, _p, ctypes.POINTER(BatchReport)]),
     "rm_batch_plan_panel_width": (ctypes.c_int, [_p, ctypes.c_int]),
     "rm_batch_plan_cta_threads": (ctypes.c_int, [_p, ctypes.c_int]),
+    "rm_batch_plan_precision": (ctypes.c_int, [_p, ctypes.c_int]),
     "rm_batch_plan_execute_host": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p, _p]),
     "rm_batch_plan_adjoint": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p]),
     "rm_dtrsm": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i64, _i64, _p, _i64, _p,

@@ -79,11 +79,20 @@ class BatchPlan:
         return (ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x.data_ptr()),
                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
 
-    def tune(self, a, b, x):
+    def tune(self, a, b, x, precision=False):
         """Times the candidate panel widths per size bucket, and the CTA size for the systems of
-        n <= 64, on these inputs; keeps the fastest. Returns the panel widths per bucket."""
-        check(_lib.load().rm_batch_plan_tune(self._h, *self._ptrs(a, b, x)), "batch tune")
+        n <= 64, on these inputs; keeps the fastest. With `precision` (a mixed plan), each bucket
+        also times float64 factors without refinement and keeps the faster route (see
+        `precision()`). Returns the panel widths per bucket."""
+        fn = _lib.load().rm_batch_plan_tune_precision if precision else _lib.load().rm_batch_plan_tune
+        check(fn(self._h, *self._ptrs(a, b, x)), "batch tune")
         return [_lib.load().rm_batch_plan_panel_width(self._h, i) for i in range(5)]
+
+    def precision(self):
+        """The route of each size bucket (n <= 32, 64, 128, 192, 256): "mixed" (float32 factors +
+        float64 refinement) or "plain" (float64 factors)."""
+        names = {_lib.RM_METHOD_PLAIN_F64: "plain", _lib.RM_METHOD_F32_IR: "mixed"}
+        return [names.get(_lib.load().rm_batch_plan_precision(self._h, i), "?") for i in range(5)]
 
     def cta_threads(self):
         """Threads per CTA (a thread per row: 64 or 256) solving each size bucket (n <= 32, 64,

@@ -47,6 +47,8 @@ struct BatchPlan {
   std::vector<int64_t> a_off, b_off, x_off, w_off;
   rm_solve_options opts{};
   int nb_bucket[5] = {16, 16, 32, 32, 32};  // panel width per size bucket (tuned)
+  int f64_bucket[5] = {0, 0, 0, 0, 0};      // 1: the bucket's systems take float64 factors (precision tuner)
+  int code(int bucket) const { return nb_bucket[bucket] | (f64_bucket[bucket] ? kItemF64 : 0); }
   // device
   int *d_sys = nullptr, *d_nb = nullptr, *d_n = nullptr, *d_k = nullptr, *d_iters = nullptr, *d_flags = nullptr,
       *d_counter = nullptr;
@@ -128,7 +130,7 @@ static int plan_build(BatchPlan* p) {
   }
   p->w_bytes = std::max<size_t>(off, 256);
   p->nb_item.resize(cnt);
-  for (int64_t i = 0; i < cnt; ++i) p->nb_item[i] = p->nb_bucket[bucket_of(p->n[p->order[i]])];
+  for (int64_t i = 0; i < cnt; ++i) p->nb_item[i] = p->code(bucket_of(p->n[p->order[i]]));
   RM_TRY(upload(&p->d_sys, p->order));
   RM_TRY(upload(&p->d_nb, p->nb_item));
   RM_TRY(upload(&p->d_n, p->n));
@@ -297,7 +299,10 @@ int batch_plan_execute(BatchPlan* p, const double* a, const double* b, double* x
 // faster stays. Then the CTA size for the systems of n <= 64: each choice of the largest n
 // that the 64-thread build takes (64, 32, or none: all on 256-thread CTAs) runs those systems
 // twice, and the fastest stays. The results are the solves of those systems (x is written).
-int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, cudaStream_t s) {
+// With `precision` (a mixed plan only), each bucket also times float64 factors without
+// refinement beside the float32 widths and keeps whichever is fastest: the systems then still
+// meet the plan's backward-error tolerance, by the float64 route.
+int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, cudaStream_t s, bool precision) {
   if (!p) return RM_BAD_ARG;
   const int cnt = (int)p->count;
   cudaEvent_t e0, e1;
@@ -311,7 +316,9 @@ int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, c
     if (first >= last) continue;
     float best = INFINITY;
     int best_nb = p->nb_bucket[bk];
-    for (int cand : {16, 32}) {
+    const bool try_f64 = precision && p->opts.method == RM_METHOD_F32_IR;
+    for (int cand : {16, 32, 16 | kItemF64}) {
+      if ((cand & kItemF64) && !try_f64) continue;
       for (int i = first; i < last; ++i) p->nb_item[i] = cand;
       if (cudaMemcpyAsync(p->d_nb + first, p->nb_item.data() + first, (last - first) * sizeof(int),
                           cudaMemcpyHostToDevice, s) != cudaSuccess) {
@@ -328,8 +335,13 @@ int batch_plan_tune(BatchPlan* p, const double* a, const double* b, double* x, c
       }
       if (t < best) best = t, best_nb = cand;
     }
-    p->nb_bucket[bk] = best_nb;
-    for (int i = first; i < last; ++i) p->nb_item[i] = best_nb;
+    if (best_nb & kItemF64) {
+      p->f64_bucket[bk] = 1;  // the float32 width stays as it was
+    } else {
+      p->f64_bucket[bk] = 0;
+      p->nb_bucket[bk] = best_nb;
+    }
+    for (int i = first; i < last; ++i) p->nb_item[i] = p->code(bk);
     if (cudaMemcpyAsync(p->d_nb + first, p->nb_item.data() + first, (last - first) * sizeof(int),
                         cudaMemcpyHostToDevice, s) != cudaSuccess)
       status = RM_CUDA_ERROR;
@@ -411,7 +423,7 @@ static int build_groups(BatchPlan* p) {
     while (sp < bounds[g + 1] && p->n[p->g_order[sp]] > p->small_limit) ++sp;
     p->g_split[g] = sp;
   }
-  for (int i = 0; i < cnt; ++i) p->g_nb[i] = p->nb_bucket[bucket_of(p->n[p->g_order[i]])];
+  for (int i = 0; i < cnt; ++i) p->g_nb[i] = p->code(bucket_of(p->n[p->g_order[i]]));
   if (!p->d_gsys) {
     RM_TRY(upload(&p->d_gsys, p->g_order));
     RM_TRY(upload(&p->d_gnb, p->g_nb));
@@ -581,7 +593,14 @@ int rm_batch_plan_create(int64_t count, const int64_t* h_n, const int64_t* h_k, 
 
 int rm_batch_plan_tune(rm_batch_plan* plan, const double* d_a, const double* d_b, double* d_x, void* stream) {
   if (!plan || !d_a || !d_b || !d_x) return RM_BAD_ARG;
-  RM_TRY(rm::batch_plan_tune(plan->p, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream)));
+  RM_TRY(rm::batch_plan_tune(plan->p, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream), false));
+  return rm::take_device_status(reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rm_batch_plan_tune_precision(rm_batch_plan* plan, const double* d_a, const double* d_b, double* d_x,
+                                 void* stream) {
+  if (!plan || !d_a || !d_b || !d_x) return RM_BAD_ARG;
+  RM_TRY(rm::batch_plan_tune(plan->p, d_a, d_b, d_x, reinterpret_cast<cudaStream_t>(stream), true));
   return rm::take_device_status(reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -616,6 +635,11 @@ int rm_batch_plan_adjoint_results(rm_batch_plan* plan, double* h_berr, double* h
 
 int rm_batch_plan_panel_width(const rm_batch_plan* plan, int bucket) {
   return plan && bucket >= 0 && bucket < 5 ? plan->p->nb_bucket[bucket] : 0;
+}
+
+int rm_batch_plan_precision(const rm_batch_plan* plan, int bucket) {
+  if (!plan || bucket < 0 || bucket >= 5) return -1;
+  return plan->p->f64_bucket[bucket] ? RM_METHOD_PLAIN_F64 : plan->p->opts.method;
 }
 
 int rm_batch_plan_cta_threads(const rm_batch_plan* plan, int bucket) {

@@ -8,10 +8,14 @@
 
 namespace rm {
 
+// An item's code in BatchArgs::nb: its float32 panel width (16 or 32) in the low byte, and
+// kItemF64 when the precision tuner gave its size bucket float64 factors (no refinement).
+constexpr int kItemF64 = 1 << 8;
+
 struct BatchArgs {
   int first, last;  // items [first, last) of the processing order
   const int* sys;   // item -> system
-  const int* nb;    // item -> panel width (16 or 32)
+  const int* nb;    // item -> panel width (16 or 32), | kItemF64 for float64 factors
   const int* n;
   const int* k;
   const int64_t* a_off;

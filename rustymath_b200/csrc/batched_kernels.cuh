@@ -784,9 +784,10 @@ __device__ void correct(Batch& bt, Smem& sm, int n, int k, int ld, const T* W, i
 
 // One system with at most KK right-hand sides (the solves and residuals loop over KK columns).
 template <int KK>
-__device__ void solve_system(Batch& bt, Smem& sm, int n, int k, int nb, int ld, const double* a, const double* b,
-                             unsigned char* w, int& my_pos, int& iters, int& flags, double& berr, bool& done) {
-  if (bt.method == RM_METHOD_F32_IR) {
+__device__ void solve_system(Batch& bt, Smem& sm, int method, int n, int k, int nb, int ld, const double* a,
+                             const double* b, unsigned char* w, int& my_pos, int& iters, int& flags, double& berr,
+                             bool& done) {
+  if (method == RM_METHOD_F32_IR) {
     float* W = reinterpret_cast<float*>(w);
     if (nb == 32) factor_and_solve<float, 32, KK>(bt, sm, n, k, ld, W, a, b, my_pos);
     else factor_and_solve<float, 16, KK>(bt, sm, n, k, ld, W, a, b, my_pos);
@@ -806,7 +807,7 @@ __device__ void solve_system(Batch& bt, Smem& sm, int n, int k, int nb, int ld, 
     }
     if (!done) flags |= bt.fallback ? FLAG_FELL_BACK : FLAG_NO_CONVERGENCE;
   }
-  if (!done && (bt.method != RM_METHOD_F32_IR || bt.fallback)) {
+  if (!done && (method != RM_METHOD_F32_IR || bt.fallback)) {
     double* W = reinterpret_cast<double*>(w);
     const bool nonzero = factor_and_solve<double, 16, KK>(bt, sm, n, k, ld, W, a, b, my_pos);
     berr = bresidual<KK>(a, b, n, k, sm);
@@ -835,7 +836,8 @@ __global__ void __launch_bounds__(THREADS, RM_BT_MIN_BLOCKS) batch_solve_kernel(
     const int item = item_s;
     __syncthreads();
     if (item >= bt.last) return;
-    const int s = bt.sys[item], nb = bt.nb[item];
+    const int s = bt.sys[item], code = bt.nb[item], nb = code & 0xff;
+    const int method = (code & kItemF64) ? RM_METHOD_PLAIN_F64 : bt.method;
     const int n = bt.n[s], k = bt.k[s];
     const int ld = (n + 3) & ~3;
     const double* a = bt.a + bt.a_off[s];
@@ -846,10 +848,10 @@ __global__ void __launch_bounds__(THREADS, RM_BT_MIN_BLOCKS) batch_solve_kernel(
     int my_pos = -1, iters = 0, flags = 0;
     double berr = 0.0;
     bool done = false;
-    if (k <= 1) solve_system<1>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
-    else if (k <= 2) solve_system<2>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
-    else if (k <= 4) solve_system<4>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
-    else solve_system<KMAX>(bt, sm, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    if (k <= 1) solve_system<1>(bt, sm, method, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    else if (k <= 2) solve_system<2>(bt, sm, method, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    else if (k <= 4) solve_system<4>(bt, sm, method, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
+    else solve_system<KMAX>(bt, sm, method, n, k, nb, ld, a, b, w, my_pos, iters, flags, berr, done);
     // x (row-major n x k) from xs, by unknown; the factors' row order and type stay for the adjoint
     for (int e = threadIdx.x; e < n * k; e += THREADS) x[e] = sm.xs[e / k][e % k];
     for (int i = threadIdx.x; i < n; i += THREADS) bt.piv[bt.p_off[s] + i] = sm.piv[i];
@@ -857,7 +859,7 @@ __global__ void __launch_bounds__(THREADS, RM_BT_MIN_BLOCKS) batch_solve_kernel(
       bt.berr[s] = berr;
       bt.iters[s] = iters;
       bt.flags[s] = flags;
-      bt.ftype[s] = (bt.method == RM_METHOD_F32_IR && (done || !bt.fallback)) ? 0 : 1;
+      bt.ftype[s] = (method == RM_METHOD_F32_IR && (done || !bt.fallback)) ? 0 : 1;
     }
     __syncthreads();
   }

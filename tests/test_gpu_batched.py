@@ -157,6 +157,48 @@ def test_tune_and_graph_replay(rb):
     plan.close()
 
 
+def test_tune_precision(rb):
+    """The tuner's precision axis: every size bucket keeps float32 factors + refinement or takes
+    float64 factors, whichever it timed faster; either way every system meets n 2^-53, the
+    float64 route's systems report no refinement steps, and the adjoint follows each system's
+    factors. A plain plan has no choice to make."""
+    import torch
+    rng = np.random.default_rng(11)
+    sizes = list(rng.integers(8, 257, 200)) + [1, 256]
+    ks = list(rng.integers(1, 5, 202))
+    As, Bs = batch(sizes, ks, shifted, seed=300)
+    plan = rb.BatchPlan(sizes, ks, method="mixed")
+    a, b = plan.pack(As, Bs, device="cuda")
+    x = torch.zeros(plan.b_size, dtype=torch.float64, device="cuda")
+    assert plan.precision() == ["mixed"] * 5
+    plan.tune(a, b, x, precision=True)
+    routes = plan.precision()
+    assert all(r in ("mixed", "plain") for r in routes)
+    plan.execute(a, b, x)
+    torch.cuda.synchronize()
+    Xs = [t.cpu().numpy() for t in plan.unpack(x)]
+    check_bar(As, Bs, Xs)
+    berr, iters, flags, rep = plan.results()
+    bounds = [32, 64, 128, 192, 256]
+    for n, it in zip(sizes, iters):
+        if routes[next(i for i, m in enumerate(bounds) if n <= m)] == "plain":
+            assert it == 0
+    assert rep.fell_back == 0
+    # the adjoint reads each system's own factor type
+    gx = torch.randn(plan.b_size, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    gb = torch.empty_like(gx)
+    plan.adjoint(a, x, gx, gb)
+    torch.cuda.synchronize()
+    for aa, g, y in zip(As, plan.unpack(gx), plan.unpack(gb)):
+        yo = np.linalg.solve(aa.T, g.cpu().numpy())
+        assert np.abs(y.cpu().numpy() - yo).max() <= 1e-12 * max(1.0, np.abs(yo).max())
+    plan.close()
+    plain = rb.BatchPlan(sizes, ks, method="plain")
+    plain.tune(a, b, x, precision=True)
+    assert plain.precision() == ["plain"] * 5
+    plain.close()
+
+
 def test_device_lists(rb):
     import torch
     As, Bs = batch([50, 130], [2, 1], shifted, seed=30)
