@@ -761,10 +761,15 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   // the end: the host waits once per call. A matrix that is not regular still gets
   // RM_NOT_REGULAR; x is then unspecified.
   RM_TRY(regular_flag_f64(w, lb.ldw, n, sc.at<double>(lb.amax), sc.at<int32_t>(lb.flag), s));
-  RM_TRY(invert_diag_blocks_f64(w, lb.ldw, false, n, sc.at<double>(lb.dinv), true, false, s));
-  tr.mark("regular");
-  RM_TRY(getrs_f64(w, lb.ldw, false, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k,
-                   sc.at<void>(os), device_status(), s));
+  if (small_solve_fits(n, k)) {  // one CTA, rustymath's single-column order
+    tr.mark("regular");
+    RM_TRY(small_solve_f64(w, lb.ldw, n, sc.at<int64_t>(lb.perm), d_b, k, d_x, s));
+  } else {
+    RM_TRY(invert_diag_blocks_f64(w, lb.ldw, false, n, sc.at<double>(lb.dinv), true, false, s));
+    tr.mark("regular");
+    RM_TRY(getrs_f64(w, lb.ldw, false, n, sc.at<int64_t>(lb.perm), sc.at<double>(lb.dinv), d_b, k, k, d_x, k,
+                     sc.at<void>(os), device_status(), s));
+  }
   tr.mark("getrs");
   if (report) {
     RM_TRY(residual_f64(d_a, n, n, d_x, k, d_b, k, k, sc.at<double>(orr), k, sc.at<double>(onorm), s));

@@ -108,6 +108,21 @@ def test_small_lu_is_the_oracles_bits(rb, n):
         assert np.array_equal(f, fo)
 
 
+@pytest.mark.parametrize("n", [1, 2, 5, 32, 33, 71, 100, 128, 191, 192])
+def test_small_solve_is_the_oracles_bits(rb, n):
+    """Up to n = 192 with one right-hand side, solve is the oracle's LuWork::solve bit for bit:
+    the factors as above, then the single-column triangular solves in rustymath's order
+    (core/src/linalg/factor.rs:725-748). With 2..8 right-hand sides each column is solved the
+    same way, within n*eps of the oracle (which takes its blocked route there)."""
+    rng = np.random.default_rng(40 + n)
+    for a in (ref_random(n, n, n + 1), rng.standard_normal((n, n)) + n * np.eye(n)):
+        b = rng.standard_normal((n, 1))
+        assert np.array_equal(rb.solve(a, b), O.solve(a, b))
+        b3 = rng.standard_normal((n, 3))
+        x3, xo3 = rb.solve(a, b3), O.solve(a, b3)
+        assert np.abs(x3 - xo3).max() <= 4 * n * EPS * np.abs(xo3).max() * np.linalg.cond(a, np.inf)
+
+
 @pytest.mark.parametrize("n", [1, 5, 33, 71, 530])
 def test_lu_solve_residuals(rb, n):
     """tests/linalg.rs:384-390: solve and inverse residuals below 4*eps*n."""
