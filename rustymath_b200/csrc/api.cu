@@ -655,6 +655,9 @@ int rm_dlu_solve(int64_t n, const double* d_factors, const int64_t* d_perm, cons
   if (!d_factors || !d_perm || !d_b || !d_x) return RM_BAD_ARG;
   RM_TRY(check_device());
   cudaStream_t s = as_stream(stream);
+  // n <= 192, k <= 8: one CTA in rustymath's single-column order, no scratch
+  if (!trans && small_solve_fits(n, k))
+    return small_solve_f64(d_factors, n, true, n, d_perm, d_b, k, d_x, device_status(), s);
   Arena ar;
   const size_t od = ar.add(diag_blocks_f64_bytes(n)), os = ar.add(getrs_f64_scratch_bytes(n, k));
   Scratch sc;
@@ -763,7 +766,7 @@ static int dsolve_plain(int64_t n, const double* d_a, const double* d_b, int64_t
   RM_TRY(regular_flag_f64(w, lb.ldw, n, sc.at<double>(lb.amax), sc.at<int32_t>(lb.flag), s));
   if (small_solve_fits(n, k)) {  // one CTA, rustymath's single-column order
     tr.mark("regular");
-    RM_TRY(small_solve_f64(w, lb.ldw, n, sc.at<int64_t>(lb.perm), d_b, k, d_x, s));
+    RM_TRY(small_solve_f64(w, lb.ldw, false, n, sc.at<int64_t>(lb.perm), d_b, k, d_x, nullptr, s));
   } else {
     RM_TRY(invert_diag_blocks_f64(w, lb.ldw, false, n, sc.at<double>(lb.dinv), true, false, s));
     tr.mark("regular");

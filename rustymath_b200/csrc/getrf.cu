@@ -644,11 +644,20 @@ constexpr int kSmallSolveK = 8;
 constexpr int kSsCols = 32;
 constexpr int kSsStride = kSsCols + 2;  // doubles per staged row (16-byte aligned rows)
 
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// COLMAJOR: the factors in rustymath's order (item (i, j) at w[j * ldw + i], exactly n columns),
+// staged as columns ([32][n] per buffer); else W row-major ([n][kSsStride] per buffer). A row
+// position outside 0..n-1 sets RM_DEV_BAD_INDEX in *status (when given) and that row's right-hand
+// side is taken as zero.
+template <bool COLMAJOR>
 __global__ void __launch_bounds__(kSmallSolveMax, 1)
     small_solve_kernel(const double* __restrict__ w, int64_t ldw, int n, const int64_t* __restrict__ perm,
-                       const double* b, int k, double* x) {
+                       const double* b, int k, double* x, unsigned* status) {
   extern __shared__ __align__(16) uint8_t smem[];
-  double* buf = reinterpret_cast<double*>(smem);  // [2][n][kSsStride]
+  double* buf = reinterpret_cast<double*>(smem);  // two staging buffers of kSsCols * kSsStride * ... doubles
   __shared__ double xs[2][kSmallSolveK];
   const int t = threadIdx.x;
   const bool own = t < n;
@@ -656,17 +665,28 @@ __global__ void __launch_bounds__(kSmallSolveMax, 1)
   double v[kSmallSolveK];
   {
     const int64_t src = own ? perm[t] : 0;
+    const bool in = src >= 0 && src < n;
+    if (own && !in && status) flag_error(status, RM_DEV_BAD_INDEX);
 #pragma unroll
-    for (int c = 0; c < kSmallSolveK; ++c) v[c] = (own && c < k) ? b[src * k + c] : 0.0;
+    for (int c = 0; c < kSmallSolveK; ++c) v[c] = (own && in && c < k) ? b[src * k + c] : 0.0;
   }
+  const size_t bufsz = COLMAJOR ? (size_t)kSsCols * n : (size_t)n * kSsStride;
   // stage q: forward blocks 0..nblk-1, then backward blocks nblk-1..0
   auto stage = [&](int q) {
     const int blk = q < nblk ? q : 2 * nblk - 1 - q;
-    double* dst = buf + (size_t)(q & 1) * n * kSsStride;
-    const double* src = w + (int64_t)blk * kSsCols;
-    for (int e = t; e < n * (kSsCols / 2); e += kSmallSolveMax) {
-      const int r = e / (kSsCols / 2), h = e % (kSsCols / 2);
-      cp_async16(dst + r * kSsStride + 2 * h, src + (int64_t)r * ldw + 2 * h);
+    double* dst = buf + (q & 1) * bufsz;
+    if constexpr (COLMAJOR) {  // columns blk*32 .. min(n, blk*32 + 32) - 1, a row item each
+      const int c0 = blk * kSsCols, cols = min(kSsCols, n - c0);
+      for (int e = t; e < cols * n; e += kSmallSolveMax) {
+        const int c = e / n, r = e % n;
+        cp_async8(dst + (size_t)c * n + r, w + (int64_t)(c0 + c) * ldw + r);
+      }
+    } else {
+      const double* src = w + (int64_t)blk * kSsCols;
+      for (int e = t; e < n * (kSsCols / 2); e += kSmallSolveMax) {
+        const int r = e / (kSsCols / 2), h = e % (kSsCols / 2);
+        cp_async16(dst + r * kSsStride + 2 * h, src + (int64_t)r * ldw + 2 * h);
+      }
     }
     cp_async_commit();
   };
@@ -675,8 +695,10 @@ __global__ void __launch_bounds__(kSmallSolveMax, 1)
     cp_async_wait<0>();
     __syncthreads();  // stage q is in; every thread is done with stage q - 1's buffer
     if (q + 1 < 2 * nblk) stage(q + 1);
-    const double* S = buf + (size_t)(q & 1) * n * kSsStride;
-    const double* mine = S + (own ? t : 0) * kSsStride;
+    const double* S = buf + (q & 1) * bufsz;
+    // item (t, c0 + i) of the staged block is mine[i * step]
+    const double* mine = COLMAJOR ? S + (own ? t : 0) : S + (own ? t : 0) * kSsStride;
+    const int step = COLMAJOR ? n : 1;
     if (q < nblk) {
       const int c0 = q * kSsCols, c1 = min(n, c0 + kSsCols);
       for (int j = c0; j < c1; ++j) {
@@ -687,7 +709,7 @@ __global__ void __launch_bounds__(kSmallSolveMax, 1)
             if (c < k) xj[c] = v[c];
         __syncthreads();
         if (own && t > j) {
-          const double l = mine[j - c0];
+          const double l = mine[(j - c0) * step];
 #pragma unroll
           for (int c = 0; c < kSmallSolveK; ++c)
             if (c < k) v[c] = fma(l, -xj[c], v[c]);
@@ -698,14 +720,14 @@ __global__ void __launch_bounds__(kSmallSolveMax, 1)
       for (int j = c1 - 1; j >= c0; --j) {
         double* xj = xs[j & 1];
         if (t == j) {  // the divisions are on the critical path: only the k columns in use
-          const double d = mine[j - c0];
+          const double d = mine[(j - c0) * step];
 #pragma unroll
           for (int c = 0; c < kSmallSolveK; ++c)
             if (c < k) xj[c] = v[c] = v[c] / d;
         }
         __syncthreads();
         if (own && t < j) {
-          const double u = mine[j - c0];
+          const double u = mine[(j - c0) * step];
 #pragma unroll
           for (int c = 0; c < kSmallSolveK; ++c)
             if (c < k) v[c] = fma(u, -xj[c], v[c]);
@@ -725,12 +747,18 @@ __global__ void __launch_bounds__(kSmallSolveMax, 1)
 constexpr int kSmallSolveRoute = 192;
 bool small_solve_fits(int64_t n, int64_t k) { return n >= 1 && n <= kSmallSolveRoute && k >= 1 && k <= kSmallSolveK; }
 
-int small_solve_f64(const double* w, int64_t ldw, int64_t n, const int64_t* perm, const double* b, int64_t k,
-                    double* x, cudaStream_t stream) {
+int small_solve_f64(const double* w, int64_t ldw, bool colmajor, int64_t n, const int64_t* perm, const double* b,
+                    int64_t k, double* x, unsigned* status, cudaStream_t stream) {
   if (n < 1 || n > kSmallSolveMax || k < 1 || k > kSmallSolveK) return RM_BAD_ARG;
-  RM_TRY(smem_attribute(small_solve_kernel, (size_t)2 * kSmallSolveMax * kSsStride * sizeof(double)));
-  small_solve_kernel<<<1, kSmallSolveMax, (size_t)2 * n * kSsStride * sizeof(double), stream>>>(
-      w, ldw, (int)n, perm, b, (int)k, x);
+  if (colmajor) {
+    RM_TRY(smem_attribute(small_solve_kernel<true>, (size_t)2 * kSsCols * kSmallSolveMax * sizeof(double)));
+    small_solve_kernel<true><<<1, kSmallSolveMax, (size_t)2 * kSsCols * n * sizeof(double), stream>>>(
+        w, ldw, (int)n, perm, b, (int)k, x, status);
+  } else {
+    RM_TRY(smem_attribute(small_solve_kernel<false>, (size_t)2 * kSmallSolveMax * kSsStride * sizeof(double)));
+    small_solve_kernel<false><<<1, kSmallSolveMax, (size_t)2 * n * kSsStride * sizeof(double), stream>>>(
+        w, ldw, (int)n, perm, b, (int)k, x, status);
+  }
   RM_LAUNCHED();
   return RM_OK;
 }

@@ -66,12 +66,14 @@ int load_matrix_f64(const double* a, int64_t lda, double* w, int64_t ldw, int64_
                     cudaStream_t stream);
 // Writes the column-major factors (item (i,j) at f[j*n+i]) from the row-major W.
 int store_factors_f64(const double* w, int64_t ldw, int64_t n, double* factors, cudaStream_t stream);
-// x = (P^T L U)^-1 b for n <= 256 and k <= 8 from W after getrf_f64, in one CTA, in rustymath's
-// single-column order; b, x row-major n x k (ld k). small_solve_fits: the sizes the plain solve
-// sends there (n <= 192, where it is the faster route).
+// x = (P^T L U)^-1 b for n <= 256 and k <= 8 in one CTA, in rustymath's single-column order, from
+// W after getrf_f64 (row-major) or from rustymath's column-major factors (colmajor, ld = ldw);
+// b, x row-major n x k (ld k). A row position outside 0..n-1 sets RM_DEV_BAD_INDEX in *status
+// (when not NULL). small_solve_fits: the sizes the solves send there (n <= 192, where it is the
+// faster route).
 bool small_solve_fits(int64_t n, int64_t k);
-int small_solve_f64(const double* w, int64_t ldw, int64_t n, const int64_t* perm, const double* b, int64_t k,
-                    double* x, cudaStream_t stream);
+int small_solve_f64(const double* w, int64_t ldw, bool colmajor, int64_t n, const int64_t* perm, const double* b,
+                    int64_t k, double* x, unsigned* status, cudaStream_t stream);
 // *flag = 1 when every |u_ii| > eps*n*amax (LuWork::regular), else 0.
 int regular_flag_f64(const double* w, int64_t ldw, int64_t n, const double* amax, int32_t* flag,
                      cudaStream_t stream);

@@ -82,16 +82,18 @@ def test_allocation_failures_are_reported(kind, status):
     _solve_ok(n, k, method="mixed")
 
 
-def test_a_bad_row_position_is_reported_by_take_status():
+@pytest.mark.parametrize("n", [100, 257])
+def test_a_bad_row_position_is_reported_by_take_status(n):
+    """n = 100 takes the one-CTA solve without a transpose, n = 257 the block-chained solves."""
     import torch
     import rustymath_b200 as rb
     _l, lib = _lib()
-    n, k = 257, 3
+    k = 3
     rng = np.random.default_rng(5)
     a = torch.tensor(rng.standard_normal((n, n)) + n * np.eye(n), device="cuda")
     fac = rb.lu(a)
     bad = fac.p.clone()
-    bad[100] = -1
+    bad[n // 2] = -1
     b = torch.tensor(rng.standard_normal((n, k)), device="cuda")
     x = torch.empty_like(b)
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)

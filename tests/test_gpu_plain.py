@@ -123,6 +123,23 @@ def test_small_solve_is_the_oracles_bits(rb, n):
         assert np.abs(x3 - xo3).max() <= 4 * n * EPS * np.abs(xo3).max() * np.linalg.cond(a, np.inf)
 
 
+@pytest.mark.parametrize("n", [1, 2, 33, 100, 192])
+def test_small_lu_solve_is_the_oracles_bits(rb, n):
+    """lu_solve from rustymath's column-major factors (Lu.solve, factor.rs:633-641) up to n = 192:
+    with one right-hand side the oracle's lu_solve bit for bit, with three within n*eps of it;
+    the transposed solve keeps the block-chained kernels."""
+    rng = np.random.default_rng(70 + n)
+    a = rng.standard_normal((n, n)) + n * np.eye(n)
+    f, p = rb.lu(a)
+    b = rng.standard_normal((n, 1))
+    assert np.array_equal(rb.lu_solve(f, p, b), O.lu_solve(f, p, b))
+    b3 = rng.standard_normal((n, 3))
+    x3, xo3 = rb.lu_solve(f, p, b3), O.lu_solve(f, p, b3)
+    assert np.abs(x3 - xo3).max() <= 4 * n * EPS * np.abs(xo3).max() * np.linalg.cond(a, np.inf)
+    xt = rb.lu_solve(f, p, b3, trans=True)
+    assert np.abs(a.T @ xt - b3).max() <= 4 * n * EPS * np.abs(a).sum(0).max() * np.abs(xt).max() + 1e-300
+
+
 @pytest.mark.parametrize("n", [1, 5, 33, 71, 530])
 def test_lu_solve_residuals(rb, n):
     """tests/linalg.rs:384-390: solve and inverse residuals below 4*eps*n."""
